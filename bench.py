@@ -1,0 +1,371 @@
+"""PSTM throughput benchmark (pairs of output sample x input trace per second).
+
+Default workload: the 3D PSTM, plain FP32 -- 500k traces x 1000 samples at 4 ms,
+midpoints uniform over 5 x 5 km, offsets uniform 0-3000 m, azimuths uniform,
+200 Ricker-30 Hz diffractors + 3 % noise, V_rms(t0, x, y) rising 1500 -> 3500
+m/s with a +-5 % lateral sinusoid, output 200 x 200 x 1000 at 25 m, 1000 m
+aperture, 60 deg angle.  Synthetic, seeded.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|bf16|f16]
+  python bench.py --impl reference ...   (CPU port of the reference kernel)
+
+One JSON line on rank 0.  ``value`` = pairs / device time of one step with the
+inputs resident in HBM (stage traces + fold + forward migration; the geometry
+plan is built once, outside the timed region), max over ranks; ``e2e`` = the same
+metric through MigrationEngine.migrate_bin_full with pinned host inputs,
+host<->device copies and plan construction inside the timed region.
+Inputs (2 GB of traces) are larger than the 126 MB L2, so no L2 flush is needed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MUFU_PER_SM_CLK = 16
+RSQRT_PER_PAIR = 2
+
+
+def peaks():
+    p = {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0, "source": "fallback"}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        p.update(hbm_gbs=float(m["hbm_gbs"]), sm_max_mhz=float(m.get("sm_max_mhz", 1965.0)),
+                 source="measured")
+    except Exception:
+        pass
+    return p
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        try:
+            p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                  "--format=csv,noheader,nounits", "-lms", "200"],
+                                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            return
+        while not self._stop.is_set():
+            line = p.stdout.readline()
+            if not line:
+                break
+            self.rows.append([x.strip() for x in line.split(",")])
+        p.terminate()
+        try:
+            p.wait(timeout=5)
+        except Exception:
+            p.kill()
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        time.sleep(0.3)
+        self._stop.set()
+        self._t.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def make_workload(device, rank: int, args):
+    from seisproc_b200 import synthetic
+    return synthetic.survey_3d(n_traces=args.traces, seed=2025 + rank, device=device,
+                               n_samples=args.samples, n_il=args.grid, n_xl=args.grid)
+
+
+def cpu_crop_columns(s, side: int):
+    """Flat column indices of a centred side x side crop of the output grid."""
+    i0 = s.n_il // 2 - side // 2
+    j0 = s.n_xl // 2 - side // 2
+    il = np.arange(i0, i0 + side)[:, None]
+    xl = np.arange(j0, j0 + side)[None, :]
+    return np.sort((il * s.n_xl + xl).ravel())
+
+
+def run_cpu_port(s, cols, fold_pairs_cols):
+    """Reference-port CPU timing on a column crop (all traces supplied)."""
+    from oracle.ref_port import engine_full_port
+    threads = len(os.sched_getaffinity(0))
+    torch.set_num_threads(threads)
+    tr = s.traces.cpu().numpy()
+    t0 = time.perf_counter()
+    engine_full_port(tr, s.source_x - s.origin_x, s.source_y - s.origin_y,
+                     s.receiver_x - s.origin_x, s.receiver_y - s.origin_y, 0.0, 0.0,
+                     s.il_spacing, s.xl_spacing, s.n_il, s.n_xl, s.dt_ms, 0.0, s.n_times,
+                     float(s.vrms.mean()), s.max_aperture_m, s.max_angle_deg,
+                     column_subset=cols)
+    el = time.perf_counter() - t0
+    return {"value": fold_pairs_cols / el / 1e9, "unit": "Gpairs/s", "cores": threads,
+            "kind": "port", "seconds": el,
+            "sample": f"centred {int(round(len(cols) ** 0.5))}x{int(round(len(cols) ** 0.5))}-column "
+                      f"crop x {s.n_times} samples, all {s.n_traces} traces supplied, "
+                      f"{fold_pairs_cols:.3e} pairs; constant V = mean V_rms"}
+
+
+def bench_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    s = make_workload("cpu" if not torch.cuda.is_available() else "cuda", 0, args)
+    from oracle import pstm_fp64 as O
+    cols = cpu_crop_columns(s, args.crop)
+    il = cols // s.n_xl
+    xl = cols % s.n_xl
+    cx = s.origin_x + il * s.il_spacing
+    cy = s.origin_y + xl * s.xl_spacing
+    t_ms = (np.arange(s.n_times, dtype=np.float32) * np.float32(s.dt_ms)).astype(np.float64)
+    pairs = O.count_pairs_fp64(s.source_x, s.source_y, s.receiver_x, s.receiver_y, cx, cy, t_ms,
+                               float(s.vrms.mean()), s.max_aperture_m, s.max_angle_deg)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = run_cpu_port(s, cols, pairs)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.median([r["value"] for r in vals])
+    ms = statistics.median([r["seconds"] for r in vals]) * 1e3
+    cb = dict(vals[0])
+    cb["value"] = v
+    cb.pop("seconds", None)
+    print(json.dumps({
+        "metric": "PSTM Gpairs/s (out-sample x trace)", "value": v, "unit": "Gpairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "3D PSTM plain FP32 (500k traces x 1000 samples, 200x200x1000 "
+                               "output, V_rms(t0,x,y), A=1000 m, 60 deg)",
+                   "traces": s.n_traces, "samples": s.n_samples},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "Gpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def bench_ours(args):
+    import torch.distributed as dist
+    from seisproc_b200 import _lib
+    from seisproc_b200.kirchhoff import PSTMPlan
+    from seisproc_b200.engine import MigrationEngine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+    L = _lib.lib()
+
+    t_gen = time.perf_counter()
+    s = make_workload(dev, rank, args)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_gen
+    n_t = s.n_times
+    vel = torch.from_numpy(s.vrms.reshape(n_t, -1)).to(dev)
+    coords = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+              for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter()
+    plan = PSTMPlan(*coords, n_il=s.n_il, n_xl=s.n_xl, n_times=n_t, origin_x=s.origin_x,
+                    origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                    xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                    in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                    max_angle_deg=s.max_angle_deg, storage=args.storage, variant=args.variant)
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter() - t_plan
+    traces = s.traces
+    image = torch.empty((n_t, s.n_il, s.n_xl), device=dev)
+    fold = torch.empty_like(image)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record()
+        plan.load_traces(traces)
+        if ev:
+            ev[1].record()
+        plan.migrate_loaded(vel, image=image, with_fold=False)
+        if ev:
+            ev[2].record()
+        f = plan.fold(vel)
+        if ev:
+            ev[3].record()
+        return f
+
+    for _ in range(args.warmup):
+        f = step()
+    plan.check()
+    pairs = float(f.double().sum().item())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    l0 = L.pstm_launch_count()
+    with ClockSampler(local) as clk:
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record()
+        for i in range(args.steps):
+            step(evs[i])
+        end.record()
+        torch.cuda.synchronize()
+    launches = L.pstm_launch_count() - l0
+    plan.check()
+    total_ms = start.elapsed_time(end)
+    stage_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    fwd_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    fold_ms = [e[2].elapsed_time(e[3]) for e in evs]
+    t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tp = torch.tensor([pairs], device=dev, dtype=torch.float64)
+        dist.all_reduce(tp)
+        pairs_all = float(tp.item())
+    else:
+        pairs_all = pairs
+    total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    value = pairs_all * args.steps / (total_ms * 1e-3) / 1e9
+
+    # e2e through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_tr = torch.empty(traces.shape, dtype=torch.float32, pin_memory=True)
+        host_tr.copy_(traces)
+        host_v = torch.empty(s.vrms.shape, dtype=torch.float32, pin_memory=True)
+        host_v.copy_(torch.from_numpy(s.vrms))
+        host_c = []
+        for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y):
+            h = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+            h.copy_(torch.from_numpy(a))
+            host_c.append(h)
+        eng = MigrationEngine(storage=args.storage, variant=args.variant)
+        kw = dict(origin_x=s.origin_x, origin_y=s.origin_y, il_spacing=s.il_spacing,
+                  xl_spacing=s.xl_spacing, azimuth_deg=0.0, n_il=s.n_il, n_xl=s.n_xl,
+                  dt_ms=s.dt_ms, t_min_ms=0.0, n_times=n_t, max_aperture_m=s.max_aperture_m,
+                  max_angle_deg=s.max_angle_deg, normalize=True)
+        run = lambda: eng.migrate_bin_full(host_tr.numpy(), *[h.numpy() for h in host_c],
+                                           velocity_model=host_v.numpy(), **kw)
+        run()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e_steps = max(1, min(args.steps, 3))
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(e_steps):
+            img_np, fold_np = run()
+        b.record()
+        torch.cuda.synchronize()
+        te = torch.tensor([a.elapsed_time(b)], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e_ms = float(te.item())
+        h2d = host_tr.numel() * 4 + sum(h.numel() * 8 for h in host_c) + host_v.numel() * 4
+        d2h = img_np.nbytes + fold_np.nbytes
+        e2e = {"value": pairs_all * e_steps / (e_ms * 1e-3) / 1e9, "unit": "Gpairs/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": e_ms / e_steps}
+
+    result = None
+    if rank == 0:
+        pk = peaks()
+        clocks = clk.summary()
+        fwd_avg = statistics.mean(fwd_ms)
+        peak_pairs = 148 * MUFU_PER_SM_CLK / RSQRT_PER_PAIR * pk["sm_max_mhz"] * 1e6 / 1e12
+        achieved = pairs / (fwd_avg * 1e-3) / 1e12
+        roof = {"bound": "mufu", "achieved": achieved, "peak": peak_pairs, "unit": "Tpairs/s",
+                "frac": achieved / peak_pairs, "traffic": None,
+                "peak_source": f"{pk['source']} sm_max_mhz {pk['sm_max_mhz']}",
+                "kernel": "pstm_gather_kernel (forward)", "kernel_ms": fwd_avg,
+                "stage_ms": statistics.mean(stage_ms), "fold_ms": statistics.mean(fold_ms)}
+        cb = None
+        if world == 1 and not args.no_cpu:
+            cols = cpu_crop_columns(s, args.crop)
+            fold_cols = float(f.reshape(n_t, -1)[:, torch.from_numpy(cols).to(dev)].double().sum())
+            cb = run_cpu_port(s, cols, fold_cols)
+            cb.pop("seconds", None)
+        result = {
+            "metric": "PSTM Gpairs/s (out-sample x trace)", "value": value, "unit": "Gpairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.storage, "data": "synthetic",
+            "config": {"workload": "3D PSTM plain FP32 (500k traces x 1000 samples, 200x200x1000 "
+                                   "output, V_rms(t0,x,y), A=1000 m, 60 deg)"
+                       if args.storage == "f32" and args.traces == 500_000 else
+                       f"3D PSTM {args.storage} storage ({args.traces} traces x {args.samples} "
+                       f"samples, {args.grid}x{args.grid}x{args.samples} output)",
+                       "traces_per_gpu": s.n_traces, "pairs_per_step_per_gpu": pairs,
+                       "plan": plan.stats(), "plan_build_s": t_plan, "datagen_s": t_gen,
+                       "l2": "inputs (traces) larger than L2; no flush",
+                       "parallelism": f"output-survey shards, {world} rank(s), no collective"},
+            "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(result), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
+    ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--traces", type=int, default=500_000)
+    ap.add_argument("--samples", type=int, default=1000)
+    ap.add_argument("--grid", type=int, default=200)
+    ap.add_argument("--crop", type=int, default=4)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_ours(args)
+
+
+if __name__ == "__main__":
+    main()

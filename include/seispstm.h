@@ -1,0 +1,209 @@
+/*
+ * seispstm.h - C ABI of the B200 Kirchhoff pre-stack time migration library
+ * (libseispstm.so, CUDA sm_100a).
+ *
+ * The library replaces the compute of SeisProc's PSTM hot path: the Python
+ * signatures it sits under are
+ *   MigrationEngine.migrate_bin_full   processors/migration/migration_engine.py:225-360
+ *   migrate_kirchhoff_full             processors/migration/kirchhoff_kernel.py:459-854
+ *   normalize_by_fold                  processors/migration/kirchhoff_kernel.py:437-456
+ *   KirchhoffMigrator._migrate_chunk   processors/migration/kirchhoff_migrator.py:256-404
+ * and the host binding that calls these entry points lives in the Python
+ * package seisproc_b200 (ctypes).  SeisProc's PSTM path has no native FFI of its
+ * own (it is pure PyTorch), so these signatures are new; each one names the
+ * reference function whose work it performs.
+ *
+ * Conventions
+ *  - Plain C types only; every array argument is a DEVICE pointer unless
+ *    stated otherwise.  `stream` is a cudaStream_t passed as void*.
+ *  - Traces are (n_samples, n_traces) sample-major float32, the reference's
+ *    layout (views/migration_monitor_dialog.py:254 transposes into it).
+ *  - Images and folds are (n_times, n_il, n_xl) float32, il-major columns
+ *    (migration_engine.py:295-301).
+ *  - Velocities are V_rms at the output samples, addressed as
+ *    velocity[k * v_stride_t + c * v_stride_c] with k the output sample and
+ *    c = il * n_xl + xl the column; both strides 0 means a constant velocity.
+ *  - No C++ exception crosses this boundary.  Every entry point returns a
+ *    pstm_status; pstm_last_error() gives the message of the last failure on
+ *    the calling thread.
+ *  - Calls are asynchronous on `stream` unless stated; a plan must not be used
+ *    by two calls that overlap in time.
+ */
+#ifndef SEISPSTM_H_
+#define SEISPSTM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SEISPSTM_ABI_VERSION 1
+
+typedef enum pstm_status {
+  PSTM_OK = 0,
+  PSTM_EINVAL = 1,   /* invalid argument or configuration (reference raises ValueError) */
+  PSTM_ENOMEM = 2,   /* device allocation failed */
+  PSTM_ETIMEOUT = 3, /* a bounded device-side wait expired; the result is invalid */
+  PSTM_EBOUNDS = 4,  /* a device-side bounds check fired; the result is invalid */
+  PSTM_ECUDA = 5,    /* CUDA runtime error */
+  PSTM_ENOTSUP = 6   /* combination not built into this library */
+} pstm_status;
+
+typedef enum pstm_dtype {
+  PSTM_F32 = 0,
+  PSTM_BF16 = 1,
+  PSTM_F16 = 2,
+  PSTM_F64 = 3
+} pstm_dtype;
+
+/* Amplitude weight (models/migration_config.py:40-45 WeightMode).
+ * OBLIQUITY_SPREADING is migrate_kirchhoff_full's weight
+ *   (z/(r_s+e)) (z/(r_r+e)) / (r_s r_r + e)          kirchhoff_kernel.py:690-693
+ * SPREADING is KirchhoffMigrator's 1/(sqrt(r_s^2 r_r^2) + e)   kirchhoff_migrator.py:378 */
+typedef enum pstm_weight {
+  PSTM_WEIGHT_OBLIQUITY_SPREADING = 0,
+  PSTM_WEIGHT_SPREADING = 1,
+  PSTM_WEIGHT_OBLIQUITY = 2,
+  PSTM_WEIGHT_NONE = 3
+} pstm_weight;
+
+/* Sample-index clamp.
+ * FULL:      idx = (t - in_t0)/in_dt clamped to [0, n_samples - 1.001]   kirchhoff_kernel.py:707-709
+ * MIGRATOR:  idx = (t - in_t0)/in_dt clamped to [0, n_samples - 2]       kirchhoff_migrator.py:381 */
+typedef enum pstm_clamp { PSTM_CLAMP_FULL = 0, PSTM_CLAMP_MIGRATOR = 1 } pstm_clamp;
+
+typedef struct pstm_grid {
+  int32_t n_il, n_xl, n_times;
+  /* world coordinates of column (il, xl):
+   *   x = origin_x + il * il_dx + xl * xl_dx,  y = origin_y + il * il_dy + xl * xl_dy
+   * migrate_bin_full's grid (azimuth ignored) is il_dx = il_spacing, xl_dy = xl_spacing. */
+  double origin_x, origin_y;
+  double il_dx, il_dy, xl_dx, xl_dy;
+  double t0_ms, dt_ms; /* output time axis: t0 = t0_ms + k * dt_ms */
+} pstm_grid;
+
+typedef struct pstm_params {
+  int32_t n_samples;           /* input samples per trace */
+  double in_t0_ms, in_dt_ms;   /* input trace time axis */
+  double max_aperture_m;       /* per-leg aperture h_s < A and h_r < A (kirchhoff_kernel.py:635) */
+  double max_angle_deg;        /* atan2(h, z + 1e-6) < theta on both legs (:670-685) */
+  int32_t time_dependent_aperture; /* A(z) = min(A, z tan theta) (:674-680) */
+  int32_t weight;              /* pstm_weight */
+  int32_t clamp;               /* pstm_clamp */
+  int32_t storage;             /* pstm_dtype of the in-kernel trace copy: F32, BF16 or F16 */
+  int32_t antialias;           /* 1: causal-integrated triangle anti-alias filter */
+  double aa_dx, aa_dy;         /* output spacing used for the operator-dip half-width */
+  double aa_max_halfwidth;     /* cap on the triangle half-width, in input samples */
+  int32_t variant;             /* kernel shape id; 0 = built-in heuristic */
+} pstm_params;
+
+typedef struct pstm_geometry {
+  int64_t n_traces;
+  int32_t coord_dtype; /* PSTM_F32 or PSTM_F64; world coordinates, device pointers */
+  const void* source_x;
+  const void* source_y;
+  const void* receiver_x;
+  const void* receiver_y;
+} pstm_geometry;
+
+typedef struct pstm_plan_stats {
+  int64_t n_traces;
+  int64_t n_tiles;
+  int64_t list_entries;     /* total (tile, trace) candidate pairs after culling */
+  int64_t device_bytes;     /* scratch owned by the plan */
+  int32_t tile_il, tile_xl; /* columns per tile */
+  int32_t t_window;         /* output samples per CTA window */
+  int32_t variant;
+} pstm_plan_stats;
+
+typedef struct pstm_plan pstm_plan;
+
+/* Library ABI version (SEISPSTM_ABI_VERSION). */
+int32_t pstm_abi_version(void);
+
+/* Copies the last error message of the calling thread into buf (NUL-terminated,
+ * truncated to n bytes); returns its full length. */
+int32_t pstm_last_error(char* buf, size_t n);
+
+/* Builds a migration plan: converts the world coordinates to grid-local float32
+ * (the grid origin is subtracted in float64), bins traces by midpoint, sorts
+ * them spatially and builds, for every output tile, the list of traces whose
+ * legs can fall inside the aperture of any of its columns.  Replaces the
+ * per-tile midpoint pre-filter of kirchhoff_kernel.py:572-602.  Allocates the
+ * plan's device scratch; synchronises `stream` once to size the lists. */
+pstm_status pstm_plan_create(pstm_plan** plan, const pstm_grid* grid, const pstm_params* params,
+                             const pstm_geometry* geometry, void* stream);
+
+pstm_status pstm_plan_destroy(pstm_plan* plan);
+
+pstm_status pstm_plan_get_stats(const pstm_plan* plan, pstm_plan_stats* stats);
+
+/* Loads traces into the plan's spatially sorted, trace-major device copy in the
+ * plan's storage dtype (per-trace float32 scale for BF16/F16; for the
+ * anti-alias filter, the trend-removed double integral).  `traces` is
+ * (n_samples, n_traces) float32, or (n_traces, n_samples) if trace_major. */
+pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace_major,
+                             void* stream);
+
+/* Forward migration (data -> image): the work of migrate_kirchhoff_full
+ * (kirchhoff_kernel.py:459-854) on the traces last loaded into the plan.
+ * image and fold are (n_times, n_il, n_xl) float32 and are overwritten.
+ * fold may be NULL. */
+pstm_status pstm_migrate_loaded(pstm_plan* plan, const float* velocity, int64_t v_stride_t,
+                                int64_t v_stride_c, float* image, float* fold, void* stream);
+
+/* pstm_load_traces + pstm_migrate_loaded in one call. */
+pstm_status pstm_migrate(pstm_plan* plan, const float* traces, int32_t trace_major,
+                         const float* velocity, int64_t v_stride_t, int64_t v_stride_c,
+                         float* image, float* fold, void* stream);
+
+/* Fold only: number of traces inside the aperture and angle masks per output
+ * sample (kirchhoff_kernel.py:724-726). */
+pstm_status pstm_fold(pstm_plan* plan, const float* velocity, int64_t v_stride_t,
+                      int64_t v_stride_c, float* fold, void* stream);
+
+/* Adjoint of pstm_migrate (image -> data, Kirchhoff demigration): scatters
+ * w * image(t0, x) into samples i0 and i0+1 of every trace inside the masks.
+ * traces_out is (n_samples, n_traces) float32 (or trace-major) and is
+ * overwritten.  No reference counterpart exists (the reference has no adjoint);
+ * it is the exact transpose of the forward operator. */
+pstm_status pstm_demigrate(pstm_plan* plan, const float* image, const float* velocity,
+                           int64_t v_stride_t, int64_t v_stride_c, float* traces_out,
+                           int32_t trace_major, void* stream);
+
+/* Gradient of <grad_image, migrate(traces; V)> with respect to V_rms at every
+ * output sample (traveltime and weight recomputed, masks held fixed), for the
+ * OBLIQUITY_SPREADING weight.  Uses the traces last loaded into the plan.
+ * grad_velocity is (n_times, n_il, n_xl) float32, overwritten. */
+pstm_status pstm_velocity_gradient(pstm_plan* plan, const float* grad_image,
+                                   const float* velocity, int64_t v_stride_t,
+                                   int64_t v_stride_c, float* grad_velocity, void* stream);
+
+/* Synchronises `stream`, then reads and clears the plan's device-side error
+ * flags: PSTM_ETIMEOUT (a bounded wait for a trace copy expired),
+ * PSTM_EBOUNDS, or PSTM_EINVAL for a velocity that is not positive and finite
+ * or whose depth V*t0/2 decreases with t0.  Results computed since the last
+ * check are invalid when this does not return PSTM_OK. */
+pstm_status pstm_check(pstm_plan* plan, void* stream);
+
+/* image / fold where fold >= min_fold, else image unchanged (out may alias image).
+ * kirchhoff_kernel.py:437-456. */
+pstm_status pstm_normalize_by_fold(const float* image, const float* fold, float* out, int64_t n,
+                                   float min_fold, void* stream);
+
+/* Divide by max(fold, min_fold) and zero where fold < min_fold:
+ * MigrationResult.apply_fold_normalization / KirchhoffMigrator.migrate_dataset
+ * (base_migrator.py:317-349, kirchhoff_migrator.py:496-501). */
+pstm_status pstm_normalize_mute(const float* image, const float* fold, float* out, int64_t n,
+                                float min_fold, void* stream);
+
+/* Number of kernel launches issued by this library since load (for accounting). */
+int64_t pstm_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SEISPSTM_H_ */

@@ -1,0 +1,14 @@
+// Instantiates the gather kernel for OP_FWD (one op per translation unit).
+#include "pstm_gather.cuh"
+
+namespace pstm {
+
+pstm_status launch_forward(Plan* p, const float* vel, int64_t vst, int64_t vsc, float* image,
+                           cudaStream_t s, std::string* why) {
+  KArgs A = make_args(p, vel, vst, vsc);
+  A.out = image;
+  cudaError_t e = dispatch_shape<OP_FWD>(p, A, needs_lowclamp(p), s);
+  return e == cudaSuccess ? PSTM_OK : cuda_fail(e, "forward kernel", why);
+}
+
+}  // namespace pstm

@@ -1,0 +1,71 @@
+// Internal (C++) view of a PSTM plan shared by the plan builder and the
+// migration kernels.  Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/seispstm.h"
+
+namespace pstm {
+
+// Kernel shape of one migration CTA: COLS columns (tile_il x tile_xl) x WPC
+// warps per column, each warp owning 64*M consecutive output samples.
+struct Shape {
+  int id;
+  int cols, wpc, m;
+  int tile_il, tile_xl;
+  int t_window() const { return wpc * 64 * m; }
+  int threads() const { return cols * wpc * 32; }
+};
+
+constexpr int kGuard = 2;        // guard entries before the first staged sample
+constexpr int kBlockTraces = 8;  // traces staged per pipeline step
+
+struct Plan {
+  int device = 0;
+  pstm_grid grid{};
+  pstm_params params{};
+  int64_t n_traces = 0;
+  int n_samples = 0;
+  int row_stride = 0;  // elements per staged trace row (multiple of 8)
+  int elt_bytes = 4;
+  Shape shape{};
+  int tiles_il = 0, tiles_xl = 0;
+  int64_t n_tiles = 0;
+  int n_windows = 0;
+  // grid-local column coordinate steps (world origin subtracted in float64)
+  float il_dx = 0, il_dy = 0, xl_dx = 0, xl_dy = 0;
+  float tan_theta = 0;
+  // device buffers
+  float4* geo = nullptr;         // (sx, sy, rx, ry) local, spatially sorted
+  int* perm = nullptr;           // sorted -> original trace index
+  int* inv_perm = nullptr;       // original -> sorted
+  int64_t* tile_off = nullptr;   // n_tiles + 1
+  int* tile_list = nullptr;      // sorted trace indices per tile
+  int64_t list_entries = 0;
+  void* traces = nullptr;        // n_traces x row_stride, storage dtype
+  float* scales = nullptr;       // per sorted trace (BF16/F16), else nullptr
+  float* accum = nullptr;        // adjoint accumulation rows (n_traces x row_stride f32)
+  int* err = nullptr;            // device error flags
+  int64_t bytes = 0;
+  bool traces_loaded = false;
+};
+
+// launchers (pstm_migrate.cu)
+pstm_status launch_forward(Plan* p, const float* vel, int64_t vst, int64_t vsc, float* image,
+                           cudaStream_t s, std::string* why);
+pstm_status launch_fold(Plan* p, const float* vel, int64_t vst, int64_t vsc, float* fold,
+                        cudaStream_t s, std::string* why);
+pstm_status launch_adjoint(Plan* p, const float* image, const float* vel, int64_t vst,
+                           int64_t vsc, cudaStream_t s, std::string* why);
+pstm_status launch_vgrad(Plan* p, const float* grad_image, const float* vel, int64_t vst,
+                         int64_t vsc, float* grad_v, cudaStream_t s, std::string* why);
+pstm_status launch_velocity_check(Plan* p, const float* vel, int64_t vst, int64_t vsc,
+                                  cudaStream_t s, std::string* why);
+bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out);
+size_t forward_smem_bytes(const Plan* p);
+void count_launch();
+
+}  // namespace pstm

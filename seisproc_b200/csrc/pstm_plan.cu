@@ -1,0 +1,774 @@
+// Plan construction (geometry binning, spatial sort, per-tile trace lists),
+// trace staging into the sorted device copy, and the C ABI entry points.
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "pstm_common.cuh"
+#include "pstm_internal.h"
+
+namespace pstm {
+int64_t launch_total();
+}
+
+using namespace pstm;
+
+static thread_local std::string g_last_error;
+
+static pstm_status fail(pstm_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
+#define CUDA_TRY(expr)                                                               \
+  do {                                                                               \
+    cudaError_t _e = (expr);                                                         \
+    if (_e != cudaSuccess)                                                           \
+      return fail(_e == cudaErrorMemoryAllocation ? PSTM_ENOMEM : PSTM_ECUDA,        \
+                  std::string(#expr) + ": " + cudaGetErrorString(_e));               \
+  } while (0)
+
+#define LAUNCH_CHECK(name)                                                           \
+  do {                                                                               \
+    count_launch();                                                                  \
+    cudaError_t _e = cudaGetLastError();                                             \
+    if (_e != cudaSuccess)                                                           \
+      return fail(PSTM_ECUDA, std::string(name) + ": " + cudaGetErrorString(_e));    \
+  } while (0)
+
+// ------------------------------------------------------------------ kernels ---
+
+// World -> grid-local float32 (origin subtracted in float64), plus midpoints.
+template <typename C>
+__global__ void geo_local_kernel(const C* sx, const C* sy, const C* rx, const C* ry, int64_t n,
+                                 double ox, double oy, float4* geo, float2* mid) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const float a = (float)((double)sx[j] - ox), b = (float)((double)sy[j] - oy);
+  const float c = (float)((double)rx[j] - ox), d = (float)((double)ry[j] - oy);
+  geo[j] = make_float4(a, b, c, d);
+  mid[j] = make_float2(0.5f * (a + c), 0.5f * (b + d));
+}
+
+__device__ __forceinline__ int ord_of(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float float_of_ord(int i) {
+  return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff);
+}
+
+// bbox[0..3] = ord(min x), ord(min y), ord(max x), ord(max y)
+__global__ void bbox_kernel(const float2* mid, int64_t n, int* bbox) {
+  float mnx = 3e38f, mny = 3e38f, mxx = -3e38f, mxy = -3e38f;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const float2 m = mid[j];
+    mnx = fminf(mnx, m.x);
+    mny = fminf(mny, m.y);
+    mxx = fmaxf(mxx, m.x);
+    mxy = fmaxf(mxy, m.y);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+    mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+    mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+    mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(bbox + 0, ord_of(mnx));
+    atomicMin(bbox + 1, ord_of(mny));
+    atomicMax(bbox + 2, ord_of(mxx));
+    atomicMax(bbox + 3, ord_of(mxy));
+  }
+}
+
+__global__ void bbox_init_kernel(int* bbox) {
+  bbox[0] = ord_of(3e38f);
+  bbox[1] = ord_of(3e38f);
+  bbox[2] = ord_of(-3e38f);
+  bbox[3] = ord_of(-3e38f);
+}
+
+struct CellGrid {
+  float x0, y0, cs;
+  int ncx, ncy;
+};
+
+__global__ void cell_key_kernel(const float2* mid, int64_t n, CellGrid cg, int* key, int* iota) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const float2 m = mid[j];
+  int cx = (int)floorf((m.x - cg.x0) / cg.cs);
+  int cy = (int)floorf((m.y - cg.y0) / cg.cs);
+  cx = min(max(cx, 0), cg.ncx - 1);
+  cy = min(max(cy, 0), cg.ncy - 1);
+  key[j] = cy * cg.ncx + cx;
+  iota[j] = (int)j;
+}
+
+// cell_start[c] = first sorted position with key >= c (c = 0..n_cells)
+__global__ void cell_start_kernel(const int* keys_sorted, int64_t n, int n_cells,
+                                  int64_t* cell_start) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > n_cells) return;
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (keys_sorted[mid] < c)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  cell_start[c] = lo;
+}
+
+__global__ void gather_geo_kernel(const float4* geo_u, const int* perm, int64_t n, float4* geo,
+                                  int* inv_perm) {
+  const int64_t jj = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (jj >= n) return;
+  const int j = perm[jj];
+  geo[jj] = geo_u[j];
+  inv_perm[j] = (int)jj;
+}
+
+struct TileGeom {
+  int n_il, n_xl, tile_il, tile_xl, tiles_xl;
+  float il_dx, il_dy, xl_dx, xl_dy;
+  float reach;  // aperture (m)
+};
+
+// Tile centre and the squared cull radius: a trace can contribute to a column
+// of the tile only if both of its legs lie within A of that column, hence within
+// A + R of the centre (R = distance from the centre to the farthest corner).
+__device__ __forceinline__ void tile_disc(const TileGeom& tg, int tile, float& cx, float& cy,
+                                          float& r2, float& rad) {
+  const int ti = tile / tg.tiles_xl, tx = tile - ti * tg.tiles_xl;
+  const int il0 = ti * tg.tile_il, il1 = min(il0 + tg.tile_il, tg.n_il) - 1;
+  const int xl0 = tx * tg.tile_xl, xl1 = min(xl0 + tg.tile_xl, tg.n_xl) - 1;
+  float px[4], py[4];
+  const int ils[4] = {il0, il1, il0, il1}, xls[4] = {xl0, xl0, xl1, xl1};
+  cx = cy = 0.f;
+  for (int q = 0; q < 4; ++q) {
+    px[q] = ils[q] * tg.il_dx + xls[q] * tg.xl_dx;
+    py[q] = ils[q] * tg.il_dy + xls[q] * tg.xl_dy;
+    cx += 0.25f * px[q];
+    cy += 0.25f * py[q];
+  }
+  float R = 0.f;
+  for (int q = 0; q < 4; ++q) R = fmaxf(R, sqrtf((px[q] - cx) * (px[q] - cx) + (py[q] - cy) * (py[q] - cy)));
+  rad = tg.reach + R;
+  const float reach = rad * 1.0001f + 1.0f;  // float rounding margin
+  r2 = reach * reach;
+  rad = reach;
+}
+
+__device__ __forceinline__ bool trace_in_disc(float4 g, float cx, float cy, float r2) {
+  const float a = g.x - cx, b = g.y - cy, c = g.z - cx, d = g.w - cy;
+  return (a * a + b * b < r2) && (c * c + d * d < r2);
+}
+
+__device__ __forceinline__ void cell_rows(const CellGrid& cg, float cx, float cy, float rad,
+                                          int& cx0, int& cx1, int& cy0, int& cy1) {
+  // a midpoint of a passing trace lies within `rad` of the centre
+  cx0 = max(0, (int)floorf((cx - rad - cg.x0) / cg.cs));
+  cx1 = min(cg.ncx - 1, (int)floorf((cx + rad - cg.x0) / cg.cs));
+  cy0 = max(0, (int)floorf((cy - rad - cg.y0) / cg.cs));
+  cy1 = min(cg.ncy - 1, (int)floorf((cy + rad - cg.y0) / cg.cs));
+}
+
+__global__ void __launch_bounds__(256) tile_count_kernel(TileGeom tg, CellGrid cg,
+                                                         const int64_t* cell_start,
+                                                         const float4* geo, int64_t* counts) {
+  const int tile = blockIdx.x;
+  float cx, cy, r2, rad;
+  tile_disc(tg, tile, cx, cy, r2, rad);
+  int x0, x1, y0, y1;
+  cell_rows(cg, cx, cy, rad, x0, x1, y0, y1);
+  int64_t cnt = 0;
+  if (x0 <= x1) {
+    for (int row = y0; row <= y1; ++row) {
+      const int64_t a = cell_start[row * cg.ncx + x0], b = cell_start[row * cg.ncx + x1 + 1];
+      for (int64_t j = a + threadIdx.x; j < b; j += blockDim.x)
+        cnt += trace_in_disc(geo[j], cx, cy, r2) ? 1 : 0;
+    }
+  }
+  using BR = cub::BlockReduce<int64_t, 256>;
+  __shared__ typename BR::TempStorage tmp;
+  const int64_t total = BR(tmp).Sum(cnt);
+  if (threadIdx.x == 0) counts[tile] = total;
+}
+
+__global__ void __launch_bounds__(256) tile_fill_kernel(TileGeom tg, CellGrid cg,
+                                                        const int64_t* cell_start,
+                                                        const float4* geo, const int64_t* off,
+                                                        int* list) {
+  const int tile = blockIdx.x;
+  float cx, cy, r2, rad;
+  tile_disc(tg, tile, cx, cy, r2, rad);
+  int x0, x1, y0, y1;
+  cell_rows(cg, cx, cy, rad, x0, x1, y0, y1);
+  using BS = cub::BlockScan<int, 256>;
+  __shared__ typename BS::TempStorage tmp;
+  __shared__ int chunk_total;
+  int64_t base = off[tile];
+  if (x0 > x1) return;
+  for (int row = y0; row <= y1; ++row) {
+    const int64_t a = cell_start[row * cg.ncx + x0], b = cell_start[row * cg.ncx + x1 + 1];
+    for (int64_t j0 = a; j0 < b; j0 += blockDim.x) {
+      const int64_t j = j0 + threadIdx.x;
+      const int flag = (j < b && trace_in_disc(geo[j], cx, cy, r2)) ? 1 : 0;
+      int pos, tot;
+      BS(tmp).ExclusiveSum(flag, pos, tot);
+      if (flag) list[base + pos] = (int)j;
+      if (threadIdx.x == 0) chunk_total = tot;
+      __syncthreads();
+      base += chunk_total;
+      __syncthreads();
+    }
+  }
+}
+
+// --------------------------------------------------------- trace staging ---
+
+__global__ void maxabs_kernel(const float* tr, int64_t n_tr, int n_s, int trace_major,
+                              const int* inv_perm, float target, float* scales) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_tr) return;
+  float m = 0.f;
+  if (trace_major) {
+    const float* row = tr + j * n_s;
+    for (int i = 0; i < n_s; ++i) m = fmaxf(m, fabsf(row[i]));
+  } else {
+    for (int i = 0; i < n_s; ++i) m = fmaxf(m, fabsf(tr[(int64_t)i * n_tr + j]));
+  }
+  scales[inv_perm[j]] = m > 0.f ? m / target : 1.0f;
+}
+
+template <typename ST>
+__device__ __forceinline__ ST convert_to(float v);
+template <>
+__device__ __forceinline__ float convert_to<float>(float v) {
+  return v;
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 convert_to<__nv_bfloat16>(float v) {
+  return __float2bfloat16_rn(v);
+}
+template <>
+__device__ __forceinline__ __half convert_to<__half>(float v) {
+  return __float2half_rn(v);
+}
+
+// (n_s, n_tr) sample-major -> sorted trace-major rows, via 32x32 shared tiles.
+template <typename ST>
+__global__ void stage_transpose_kernel(const float* tr, int64_t n_tr, int n_s, const int* inv_perm,
+                                       const float* scales, int S, ST* out) {
+  __shared__ float tile[32][33];
+  const int64_t j0 = (int64_t)blockIdx.x * 32;
+  const int i0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r;
+    const int64_t j = j0 + threadIdx.x;
+    tile[r][threadIdx.x] = (i < n_s && j < n_tr) ? tr[(int64_t)i * n_tr + j] : 0.f;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t j = j0 + r;
+    const int i = i0 + threadIdx.x;
+    if (j < n_tr && i < n_s) {
+      const int jj = inv_perm[j];
+      const float inv = scales ? 1.0f / scales[jj] : 1.0f;
+      out[(int64_t)jj * S + i] = convert_to<ST>(tile[threadIdx.x][r] * inv);
+    }
+  }
+}
+
+template <typename ST>
+__global__ void stage_rows_kernel(const float* tr, int64_t n_tr, int n_s, const int* perm,
+                                  const float* scales, int S, ST* out) {
+  const int64_t jj = blockIdx.x;
+  const int j = perm[jj];
+  const float inv = scales ? 1.0f / scales[jj] : 1.0f;
+  for (int i = threadIdx.x; i < n_s; i += blockDim.x)
+    out[jj * S + i] = convert_to<ST>(tr[(int64_t)j * n_s + i] * inv);
+}
+
+// sorted trace-major accumulation rows -> caller layout, original order
+__global__ void unstage_transpose_kernel(const float* acc, int64_t n_tr, int n_s,
+                                         const int* inv_perm, int S, float* out) {
+  __shared__ float tile[32][33];
+  const int64_t j0 = (int64_t)blockIdx.x * 32;
+  const int i0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t j = j0 + r;
+    const int i = i0 + threadIdx.x;
+    tile[r][threadIdx.x] = (j < n_tr && i < n_s) ? acc[(int64_t)inv_perm[j] * S + i] : 0.f;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r;
+    const int64_t j = j0 + threadIdx.x;
+    if (i < n_s && j < n_tr) out[(int64_t)i * n_tr + j] = tile[threadIdx.x][r];
+  }
+}
+
+__global__ void unstage_rows_kernel(const float* acc, int64_t n_tr, int n_s, const int* inv_perm,
+                                    int S, float* out) {
+  const int64_t j = blockIdx.x;
+  const int jj = inv_perm[j];
+  for (int i = threadIdx.x; i < n_s; i += blockDim.x) out[j * n_s + i] = acc[(int64_t)jj * S + i];
+}
+
+__global__ void normalize_kernel(const float* image, const float* fold, float* out, int64_t n,
+                                 float min_fold, int mute) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float f = fold[i], v = image[i];
+  if (mute) {
+    out[i] = f >= min_fold ? v / fmaxf(f, min_fold) : 0.f;
+  } else {
+    out[i] = f >= min_fold ? v / f : v;
+  }
+}
+
+// ------------------------------------------------------------------ host ---
+
+static int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+template <typename T>
+static cudaError_t dalloc(Plan* p, T** ptr, size_t count) {
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(ptr), bytes);
+  if (e == cudaSuccess) p->bytes += (int64_t)bytes;
+  return e;
+}
+
+static void free_plan(Plan* p) {
+  if (!p) return;
+  cudaFree(p->geo);
+  cudaFree(p->perm);
+  cudaFree(p->inv_perm);
+  cudaFree(p->tile_off);
+  cudaFree(p->tile_list);
+  cudaFree(p->traces);
+  cudaFree(p->scales);
+  cudaFree(p->accum);
+  cudaFree(p->err);
+  delete p;
+}
+
+static pstm_status validate(const pstm_grid* g, const pstm_params* prm, const pstm_geometry* geo) {
+  if (!g || !prm || !geo) return fail(PSTM_EINVAL, "null grid/params/geometry");
+  if (g->n_il < 1 || g->n_xl < 1 || g->n_times < 1)
+    return fail(PSTM_EINVAL, "output grid dimensions must be positive");
+  if (!(g->dt_ms > 0)) return fail(PSTM_EINVAL, "output dt must be positive");
+  if (prm->n_samples < 2) return fail(PSTM_EINVAL, "traces need at least 2 samples");
+  if (!(prm->in_dt_ms > 0)) return fail(PSTM_EINVAL, "input dt must be positive");
+  if (!(prm->max_aperture_m > 0)) return fail(PSTM_EINVAL, "max_aperture_m must be positive");
+  if (!(prm->max_angle_deg > 0 && prm->max_angle_deg <= 90))
+    return fail(PSTM_EINVAL, "max_angle_deg must be in (0, 90]");
+  if (prm->weight < 0 || prm->weight > 3) return fail(PSTM_EINVAL, "unknown weight mode");
+  if (prm->clamp < 0 || prm->clamp > 1) return fail(PSTM_EINVAL, "unknown clamp mode");
+  if (prm->storage != PSTM_F32 && prm->storage != PSTM_BF16 && prm->storage != PSTM_F16)
+    return fail(PSTM_EINVAL, "storage must be F32, BF16 or F16");
+  if (prm->antialias) return fail(PSTM_ENOTSUP, "anti-alias filter is not built into this library");
+  if (geo->n_traces < 0 || geo->n_traces > (int64_t)INT32_MAX)
+    return fail(PSTM_EINVAL, "n_traces out of range");
+  if (geo->n_traces > 0 && (!geo->source_x || !geo->source_y || !geo->receiver_x || !geo->receiver_y))
+    return fail(PSTM_EINVAL, "null coordinate pointer");
+  if (geo->coord_dtype != PSTM_F32 && geo->coord_dtype != PSTM_F64)
+    return fail(PSTM_EINVAL, "coordinates must be F32 or F64");
+  const double n_out = (double)g->n_il * g->n_xl * g->n_times;
+  if (n_out > 9.0e18) return fail(PSTM_EINVAL, "output grid too large");
+  return PSTM_OK;
+}
+
+extern "C" {
+
+int32_t pstm_abi_version(void) { return SEISPSTM_ABI_VERSION; }
+
+int32_t pstm_last_error(char* buf, size_t n) {
+  if (buf && n > 0) {
+    const size_t k = std::min(n - 1, g_last_error.size());
+    memcpy(buf, g_last_error.data(), k);
+    buf[k] = '\0';
+  }
+  return (int32_t)g_last_error.size();
+}
+
+int64_t pstm_launch_count(void) { return launch_total(); }
+
+pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_params* prm,
+                             const pstm_geometry* geo, void* stream) {
+  if (!out) return fail(PSTM_EINVAL, "null plan pointer");
+  *out = nullptr;
+  pstm_status st = validate(g, prm, geo);
+  if (st != PSTM_OK) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  Plan* p = new (std::nothrow) Plan();
+  if (!p) return fail(PSTM_ENOMEM, "host allocation failed");
+  struct Guard {
+    Plan*& p;
+    bool keep = false;
+    ~Guard() {
+      if (!keep) free_plan(p);
+    }
+  } guard{p};
+  CUDA_TRY(cudaGetDevice(&p->device));
+  p->grid = *g;
+  p->params = *prm;
+  p->n_traces = geo->n_traces;
+  p->n_samples = prm->n_samples;
+  p->row_stride = (int)align_up(prm->n_samples, 8);
+  p->elt_bytes = prm->storage == PSTM_F32 ? 4 : 2;
+  if (!shape_for_variant(prm->variant, g->n_xl, g->n_times, &p->shape))
+    return fail(PSTM_EINVAL, "unknown kernel variant");
+  p->tiles_il = (g->n_il + p->shape.tile_il - 1) / p->shape.tile_il;
+  p->tiles_xl = (g->n_xl + p->shape.tile_xl - 1) / p->shape.tile_xl;
+  p->n_tiles = (int64_t)p->tiles_il * p->tiles_xl;
+  p->n_windows = (g->n_times + p->shape.t_window() - 1) / p->shape.t_window();
+  if (p->n_tiles > INT32_MAX || p->n_windows > 65535) return fail(PSTM_EINVAL, "grid too large");
+  p->il_dx = (float)g->il_dx;
+  p->il_dy = (float)g->il_dy;
+  p->xl_dx = (float)g->xl_dx;
+  p->xl_dy = (float)g->xl_dy;
+  p->tan_theta = (float)std::tan(prm->max_angle_deg * M_PI / 180.0);
+  const size_t smem = forward_smem_bytes(p);
+  if (smem > 227 * 1024)
+    return fail(PSTM_EINVAL, "traces too long for the staged kernel (" +
+                                 std::to_string(prm->n_samples) + " samples)");
+  CUDA_TRY(dalloc(p, &p->err, 4));
+  CUDA_TRY(cudaMemsetAsync(p->err, 0, 16, s));
+  CUDA_TRY(dalloc(p, &p->tile_off, p->n_tiles + 1));
+  const int64_t n = p->n_traces;
+  if (n == 0) {
+    CUDA_TRY(cudaMemsetAsync(p->tile_off, 0, (p->n_tiles + 1) * sizeof(int64_t), s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    guard.keep = true;
+    *out = reinterpret_cast<pstm_plan*>(p);
+    return PSTM_OK;
+  }
+  // temporaries
+  float4* geo_u = nullptr;
+  float2* mid = nullptr;
+  int *key = nullptr, *key_sorted = nullptr, *iota = nullptr, *bbox = nullptr;
+  int64_t *cell_start = nullptr, *counts = nullptr;
+  void* cub_tmp = nullptr;
+  struct Tmp {
+    void** ptrs[9];
+    ~Tmp() {
+      for (auto pp : ptrs)
+        if (pp && *pp) cudaFree(*pp);
+    }
+  } tmp{{(void**)&geo_u, (void**)&mid, (void**)&key, (void**)&key_sorted, (void**)&iota,
+         (void**)&bbox, (void**)&cell_start, (void**)&counts, (void**)&cub_tmp}};
+  CUDA_TRY(cudaMalloc(&geo_u, n * sizeof(float4)));
+  CUDA_TRY(cudaMalloc(&mid, n * sizeof(float2)));
+  CUDA_TRY(cudaMalloc(&key, n * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&key_sorted, n * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&iota, n * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&bbox, 4 * sizeof(int)));
+  CUDA_TRY(dalloc(p, &p->geo, n));
+  CUDA_TRY(dalloc(p, &p->perm, n));
+  CUDA_TRY(dalloc(p, &p->inv_perm, n));
+  const int thr = 256;
+  const unsigned nblk = (unsigned)((n + thr - 1) / thr);
+  if (geo->coord_dtype == PSTM_F64) {
+    geo_local_kernel<double><<<nblk, thr, 0, s>>>(
+        (const double*)geo->source_x, (const double*)geo->source_y,
+        (const double*)geo->receiver_x, (const double*)geo->receiver_y, n, g->origin_x,
+        g->origin_y, geo_u, mid);
+  } else {
+    geo_local_kernel<float><<<nblk, thr, 0, s>>>(
+        (const float*)geo->source_x, (const float*)geo->source_y, (const float*)geo->receiver_x,
+        (const float*)geo->receiver_y, n, g->origin_x, g->origin_y, geo_u, mid);
+  }
+  LAUNCH_CHECK("geo_local_kernel");
+  bbox_init_kernel<<<1, 1, 0, s>>>(bbox);
+  LAUNCH_CHECK("bbox_init_kernel");
+  bbox_kernel<<<std::min<unsigned>(nblk, 1184), thr, 0, s>>>(mid, n, bbox);
+  LAUNCH_CHECK("bbox_kernel");
+  int hb[4];
+  CUDA_TRY(cudaMemcpyAsync(hb, bbox, sizeof(hb), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  auto unord = [](int i) {
+    int v = i >= 0 ? i : i ^ 0x7fffffff;
+    float f;
+    memcpy(&f, &v, 4);
+    return f;
+  };
+  const float mnx = unord(hb[0]), mny = unord(hb[1]), mxx = unord(hb[2]), mxy = unord(hb[3]);
+  if (!std::isfinite(mnx) || !std::isfinite(mny) || !std::isfinite(mxx) || !std::isfinite(mxy))
+    return fail(PSTM_EINVAL, "non-finite trace coordinates");
+  // cell grid over the midpoints
+  const double tile_ext = std::hypot(p->shape.tile_il * std::hypot(g->il_dx, g->il_dy),
+                                     p->shape.tile_xl * std::hypot(g->xl_dx, g->xl_dy));
+  double cs = std::max(10.0, (prm->max_aperture_m + 0.5 * tile_ext) / 4.0);
+  const double ex = std::max(1.0, (double)mxx - mnx), ey = std::max(1.0, (double)mxy - mny);
+  while ((std::floor(ex / cs) + 1) * (std::floor(ey / cs) + 1) > (double)(1 << 22)) cs *= 2.0;
+  CellGrid cg;
+  cg.x0 = mnx;
+  cg.y0 = mny;
+  cg.cs = (float)cs;
+  cg.ncx = (int)std::floor(ex / cs) + 1;
+  cg.ncy = (int)std::floor(ey / cs) + 1;
+  const int n_cells = cg.ncx * cg.ncy;
+  cell_key_kernel<<<nblk, thr, 0, s>>>(mid, n, cg, key, iota);
+  LAUNCH_CHECK("cell_key_kernel");
+  int end_bit = 1;
+  while ((1 << end_bit) <= n_cells && end_bit < 31) ++end_bit;
+  size_t tmp_bytes = 0;
+  CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key, key_sorted, iota, p->perm,
+                                           (int)n, 0, end_bit, s));
+  size_t scan_bytes = 0;
+  CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (int64_t*)nullptr,
+                                         (int64_t*)nullptr, (int)(p->n_tiles + 1), s));
+  tmp_bytes = std::max(tmp_bytes, scan_bytes);
+  CUDA_TRY(cudaMalloc(&cub_tmp, tmp_bytes));
+  CUDA_TRY(cub::DeviceRadixSort::SortPairs(cub_tmp, tmp_bytes, key, key_sorted, iota, p->perm,
+                                           (int)n, 0, end_bit, s));
+  count_launch();
+  CUDA_TRY(cudaMalloc(&cell_start, (n_cells + 1) * sizeof(int64_t)));
+  cell_start_kernel<<<(n_cells + 1 + thr - 1) / thr, thr, 0, s>>>(key_sorted, n, n_cells,
+                                                                   cell_start);
+  LAUNCH_CHECK("cell_start_kernel");
+  gather_geo_kernel<<<nblk, thr, 0, s>>>(geo_u, p->perm, n, p->geo, p->inv_perm);
+  LAUNCH_CHECK("gather_geo_kernel");
+  TileGeom tg;
+  tg.n_il = g->n_il;
+  tg.n_xl = g->n_xl;
+  tg.tile_il = p->shape.tile_il;
+  tg.tile_xl = p->shape.tile_xl;
+  tg.tiles_xl = p->tiles_xl;
+  tg.il_dx = p->il_dx;
+  tg.il_dy = p->il_dy;
+  tg.xl_dx = p->xl_dx;
+  tg.xl_dy = p->xl_dy;
+  tg.reach = (float)prm->max_aperture_m;
+  CUDA_TRY(cudaMalloc(&counts, (p->n_tiles + 1) * sizeof(int64_t)));
+  CUDA_TRY(cudaMemsetAsync(counts, 0, (p->n_tiles + 1) * sizeof(int64_t), s));
+  tile_count_kernel<<<(unsigned)p->n_tiles, 256, 0, s>>>(tg, cg, cell_start, p->geo, counts);
+  LAUNCH_CHECK("tile_count_kernel");
+  CUDA_TRY(cub::DeviceScan::ExclusiveSum(cub_tmp, tmp_bytes, counts, p->tile_off,
+                                         (int)(p->n_tiles + 1), s));
+  count_launch();
+  int64_t total = 0;
+  CUDA_TRY(cudaMemcpyAsync(&total, p->tile_off + p->n_tiles, sizeof(int64_t),
+                           cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  p->list_entries = total;
+  CUDA_TRY(dalloc(p, &p->tile_list, total));
+  if (total > 0) {
+    tile_fill_kernel<<<(unsigned)p->n_tiles, 256, 0, s>>>(tg, cg, cell_start, p->geo, p->tile_off,
+                                                          p->tile_list);
+    LAUNCH_CHECK("tile_fill_kernel");
+  }
+  CUDA_TRY(cudaStreamSynchronize(s));
+  guard.keep = true;
+  *out = reinterpret_cast<pstm_plan*>(p);
+  return PSTM_OK;
+}
+
+pstm_status pstm_plan_destroy(pstm_plan* plan) {
+  free_plan(reinterpret_cast<Plan*>(plan));
+  return PSTM_OK;
+}
+
+pstm_status pstm_plan_get_stats(const pstm_plan* plan, pstm_plan_stats* st) {
+  if (!plan || !st) return fail(PSTM_EINVAL, "null argument");
+  const Plan* p = reinterpret_cast<const Plan*>(plan);
+  st->n_traces = p->n_traces;
+  st->n_tiles = p->n_tiles;
+  st->list_entries = p->list_entries;
+  st->device_bytes = p->bytes;
+  st->tile_il = p->shape.tile_il;
+  st->tile_xl = p->shape.tile_xl;
+  st->t_window = p->shape.t_window();
+  st->variant = p->shape.id;
+  return PSTM_OK;
+}
+
+pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace_major,
+                             void* stream) {
+  if (!plan) return fail(PSTM_EINVAL, "null plan");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int64_t n = p->n_traces;
+  const int n_s = p->n_samples;
+  if (n == 0) {
+    p->traces_loaded = true;
+    return PSTM_OK;
+  }
+  if (!traces) return fail(PSTM_EINVAL, "null traces");
+  if (!p->traces) {
+    const size_t bytes = (size_t)n * p->row_stride * p->elt_bytes;
+    CUDA_TRY(cudaMalloc(&p->traces, bytes));
+    p->bytes += (int64_t)bytes;
+    CUDA_TRY(cudaMemsetAsync(p->traces, 0, bytes, s));
+    if (p->params.storage != PSTM_F32) CUDA_TRY(dalloc(p, &p->scales, n));
+  }
+  const int thr = 256;
+  if (p->params.storage != PSTM_F32) {
+    const float target = p->params.storage == PSTM_F16 ? 32768.0f : 1.0f;
+    maxabs_kernel<<<(unsigned)((n + thr - 1) / thr), thr, 0, s>>>(traces, n, n_s, trace_major,
+                                                                  p->inv_perm, target, p->scales);
+    LAUNCH_CHECK("maxabs_kernel");
+  }
+  dim3 tb(32, 8);
+  dim3 tg((unsigned)((n + 31) / 32), (unsigned)((n_s + 31) / 32));
+#define PSTM_STAGE(T)                                                                          \
+  if (trace_major)                                                                             \
+    stage_rows_kernel<T><<<(unsigned)n, 256, 0, s>>>(traces, n, n_s, p->perm, p->scales,      \
+                                                     p->row_stride, (T*)p->traces);            \
+  else                                                                                         \
+    stage_transpose_kernel<T><<<tg, tb, 0, s>>>(traces, n, n_s, p->inv_perm, p->scales,       \
+                                                p->row_stride, (T*)p->traces);
+  if (p->params.storage == PSTM_F32) {
+    PSTM_STAGE(float)
+  } else if (p->params.storage == PSTM_BF16) {
+    PSTM_STAGE(__nv_bfloat16)
+  } else {
+    PSTM_STAGE(__half)
+  }
+#undef PSTM_STAGE
+  LAUNCH_CHECK("stage kernel");
+  p->traces_loaded = true;
+  return PSTM_OK;
+}
+
+static pstm_status check_velocity_args(const float* vel, int64_t vst, int64_t vsc) {
+  if (!vel) return fail(PSTM_EINVAL, "null velocity");
+  if (vst < 0 || vsc < 0) return fail(PSTM_EINVAL, "negative velocity stride");
+  return PSTM_OK;
+}
+
+pstm_status pstm_migrate_loaded(pstm_plan* plan, const float* vel, int64_t vst, int64_t vsc,
+                                float* image, float* fold, void* stream) {
+  if (!plan || !image) return fail(PSTM_EINVAL, "null plan or image");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  if (!p->traces_loaded) return fail(PSTM_EINVAL, "no traces loaded into the plan");
+  pstm_status st = check_velocity_args(vel, vst, vsc);
+  if (st != PSTM_OK) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  std::string why;
+  st = launch_velocity_check(p, vel, vst, vsc, s, &why);
+  if (st != PSTM_OK) return fail(st, why);
+  st = launch_forward(p, vel, vst, vsc, image, s, &why);
+  if (st != PSTM_OK) return fail(st, why);
+  if (fold) {
+    st = launch_fold(p, vel, vst, vsc, fold, s, &why);
+    if (st != PSTM_OK) return fail(st, why);
+  }
+  return PSTM_OK;
+}
+
+pstm_status pstm_migrate(pstm_plan* plan, const float* traces, int32_t trace_major,
+                         const float* vel, int64_t vst, int64_t vsc, float* image, float* fold,
+                         void* stream) {
+  pstm_status st = pstm_load_traces(plan, traces, trace_major, stream);
+  if (st != PSTM_OK) return st;
+  return pstm_migrate_loaded(plan, vel, vst, vsc, image, fold, stream);
+}
+
+pstm_status pstm_fold(pstm_plan* plan, const float* vel, int64_t vst, int64_t vsc, float* fold,
+                      void* stream) {
+  if (!plan || !fold) return fail(PSTM_EINVAL, "null plan or fold");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  pstm_status st = check_velocity_args(vel, vst, vsc);
+  if (st != PSTM_OK) return st;
+  std::string why;
+  st = launch_fold(p, vel, vst, vsc, fold, reinterpret_cast<cudaStream_t>(stream), &why);
+  return st == PSTM_OK ? PSTM_OK : fail(st, why);
+}
+
+pstm_status pstm_demigrate(pstm_plan* plan, const float* image, const float* vel, int64_t vst,
+                           int64_t vsc, float* traces_out, int32_t trace_major, void* stream) {
+  if (!plan || !image || !traces_out) return fail(PSTM_EINVAL, "null argument");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  pstm_status st = check_velocity_args(vel, vst, vsc);
+  if (st != PSTM_OK) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int64_t n = p->n_traces;
+  const int n_s = p->n_samples;
+  if (n == 0) return PSTM_OK;
+  if (!p->accum) CUDA_TRY(dalloc(p, &p->accum, (size_t)n * p->row_stride));
+  CUDA_TRY(cudaMemsetAsync(p->accum, 0, (size_t)n * p->row_stride * sizeof(float), s));
+  std::string why;
+  st = launch_velocity_check(p, vel, vst, vsc, s, &why);
+  if (st != PSTM_OK) return fail(st, why);
+  st = launch_adjoint(p, image, vel, vst, vsc, s, &why);
+  if (st != PSTM_OK) return fail(st, why);
+  if (trace_major) {
+    unstage_rows_kernel<<<(unsigned)n, 256, 0, s>>>(p->accum, n, n_s, p->inv_perm, p->row_stride,
+                                                    traces_out);
+  } else {
+    dim3 tb(32, 8);
+    dim3 tg((unsigned)((n + 31) / 32), (unsigned)((n_s + 31) / 32));
+    unstage_transpose_kernel<<<tg, tb, 0, s>>>(p->accum, n, n_s, p->inv_perm, p->row_stride,
+                                               traces_out);
+  }
+  LAUNCH_CHECK("unstage kernel");
+  return PSTM_OK;
+}
+
+pstm_status pstm_velocity_gradient(pstm_plan* plan, const float* grad_image, const float* vel,
+                                   int64_t vst, int64_t vsc, float* grad_v, void* stream) {
+  if (!plan || !grad_image || !grad_v) return fail(PSTM_EINVAL, "null argument");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  if (!p->traces_loaded) return fail(PSTM_EINVAL, "no traces loaded into the plan");
+  if (p->params.weight != PSTM_WEIGHT_OBLIQUITY_SPREADING)
+    return fail(PSTM_ENOTSUP, "velocity gradient is built for the obliquity x spreading weight");
+  pstm_status st = check_velocity_args(vel, vst, vsc);
+  if (st != PSTM_OK) return st;
+  std::string why;
+  st = launch_vgrad(p, grad_image, vel, vst, vsc, grad_v, reinterpret_cast<cudaStream_t>(stream),
+                    &why);
+  return st == PSTM_OK ? PSTM_OK : fail(st, why);
+}
+
+pstm_status pstm_check(pstm_plan* plan, void* stream) {
+  if (!plan) return fail(PSTM_EINVAL, "null plan");
+  Plan* p = reinterpret_cast<Plan*>(plan);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int flags = 0;
+  CUDA_TRY(cudaMemcpyAsync(&flags, p->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (flags) CUDA_TRY(cudaMemsetAsync(p->err, 0, sizeof(int), s));
+  if (flags & PSTM_ERR_TIMEOUT)
+    return fail(PSTM_ETIMEOUT, "a bounded device-side wait for a trace copy expired");
+  if (flags & PSTM_ERR_BOUNDS) return fail(PSTM_EBOUNDS, "device-side bounds check fired");
+  if (flags & PSTM_ERR_VELOCITY)
+    return fail(PSTM_EINVAL,
+                "velocity must be positive and finite with V*t0 non-decreasing in t0 per column");
+  return PSTM_OK;
+}
+
+static pstm_status normalize_common(const float* image, const float* fold, float* out, int64_t n,
+                                    float min_fold, int mute, void* stream) {
+  if (n < 0 || (n > 0 && (!image || !fold || !out))) return fail(PSTM_EINVAL, "bad arguments");
+  if (n == 0) return PSTM_OK;
+  const int thr = 256;
+  normalize_kernel<<<(unsigned)((n + thr - 1) / thr), thr, 0,
+                     reinterpret_cast<cudaStream_t>(stream)>>>(image, fold, out, n, min_fold,
+                                                               mute);
+  LAUNCH_CHECK("normalize_kernel");
+  return PSTM_OK;
+}
+
+pstm_status pstm_normalize_by_fold(const float* image, const float* fold, float* out, int64_t n,
+                                   float min_fold, void* stream) {
+  return normalize_common(image, fold, out, n, min_fold, 0, stream);
+}
+
+pstm_status pstm_normalize_mute(const float* image, const float* fold, float* out, int64_t n,
+                                float min_fold, void* stream) {
+  return normalize_common(image, fold, out, n, min_fold, 1, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,178 @@
+"""GPU parity of the sm_100a PSTM kernels against the reference's own outputs
+(golden fixtures made by running it) and against the FP64 oracle.
+
+Tolerances: FP32 image within 1e-4 relative L2 of the reference (the target
+for plain FP32); fold equal to the reference's except for pairs that sit
+within float32 rounding of a mask boundary (at most 1e-5 of all pairs).
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden_grid, load_golden, rel_l2
+from oracle import pstm_fp64 as O
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-4
+FOLD_FLIP_FRAC = 1e-5
+
+
+def _engine():
+    from seisproc_b200.engine import MigrationEngine
+    return MigrationEngine()
+
+
+def _run_golden(name):
+    d = load_golden(name)
+    g = golden_grid(d)
+    nt = int(d["n_times"])
+    img, fold = _engine().migrate_bin_full(
+        traces=d["traces"], source_x=d["source_x"], source_y=d["source_y"],
+        receiver_x=d["receiver_x"], receiver_y=d["receiver_y"], origin_x=g["origin_x"],
+        origin_y=g["origin_y"], il_spacing=g["il_spacing"], xl_spacing=g["xl_spacing"],
+        azimuth_deg=0.0, n_il=g["n_il"], n_xl=g["n_xl"], dt_ms=g["dt_ms"],
+        t_min_ms=g["t_min_ms"], n_times=nt, velocity_mps=g["velocity_mps"],
+        max_aperture_m=g["max_aperture_m"], max_angle_deg=g["max_angle_deg"], normalize=False,
+        use_time_dependent_aperture=bool(d["tda"]))
+    return d, img, fold
+
+
+@pytest.mark.parametrize("name", ["full_2d_small", "full_2d_tda_tmin", "full_3d_mini"])
+def test_engine_matches_reference_golden(name):
+    d, img, fold = _run_golden(name)
+    assert img.shape == d["image"].shape
+    err = rel_l2(img, d["image"])
+    flips = np.abs(fold - d["fold"]).sum()
+    assert err <= FP32_TOL, f"{name}: rel-L2 {err:.3e}"
+    assert flips <= max(2, FOLD_FLIP_FRAC * d["fold"].sum()), f"{name}: {flips} fold flips"
+
+
+def test_full_2d_config_matches_reference():
+    """The full-size 2D workload (2880 traces x 501 samples -> 240 x 501)."""
+    import hashlib
+    from seisproc_b200 import synthetic
+    ref = load_golden("full_2d_config")
+    s = synthetic.survey_2d(seed=1234)
+    tr = s.traces.cpu().numpy()
+    assert hashlib.sha256(tr.astype(np.float32).tobytes()).hexdigest() == str(ref["input_sha256"])
+    img, fold = _engine().migrate_bin_full(
+        traces=tr, source_x=s.source_x, source_y=s.source_y, receiver_x=s.receiver_x,
+        receiver_y=s.receiver_y, origin_x=s.origin_x, origin_y=s.origin_y,
+        il_spacing=s.il_spacing, xl_spacing=s.xl_spacing, azimuth_deg=0.0, n_il=s.n_il,
+        n_xl=s.n_xl, dt_ms=s.dt_ms, t_min_ms=s.t_min_ms, n_times=s.n_times,
+        velocity_mps=s.velocity_mps, max_aperture_m=s.max_aperture_m,
+        max_angle_deg=s.max_angle_deg, normalize=False)
+    err = rel_l2(img, ref["image"])
+    flips = np.abs(fold - ref["fold"]).sum()
+    assert err <= FP32_TOL, err
+    assert flips <= FOLD_FLIP_FRAC * ref["fold"].sum(), flips
+
+
+def _small_3d(seed=3, n_traces=4000, lateral=True, utm=(0.0, 0.0), n_samples=200):
+    from seisproc_b200 import synthetic
+    return synthetic.survey_3d(n_traces=n_traces, seed=seed, n_samples=n_samples, extent=1600.0,
+                               max_offset=1200.0, n_il=12, n_xl=10, spacing=25.0,
+                               n_diffractors=12, aperture=500.0, lateral_velocity=lateral,
+                               utm_origin=utm)
+
+
+def _oracle_3d(s, **kw):
+    n_t = s.n_times
+    il = np.arange(s.n_il)[:, None]
+    xl = np.arange(s.n_xl)[None, :]
+    cx = (s.origin_x + il * s.il_spacing + 0 * xl).ravel()
+    cy = (s.origin_y + 0 * il + xl * s.xl_spacing).ravel()
+    t_ms = (np.arange(n_t, dtype=np.float32) * np.float32(s.dt_ms)).astype(np.float64)
+    v = s.vrms.reshape(n_t, -1).astype(np.float64)
+    return O.migrate_fp64(s.traces.cpu().numpy(), s.source_x, s.source_y, s.receiver_x,
+                          s.receiver_y, cx, cy, t_ms, v, s.dt_ms, 0.0, s.max_aperture_m,
+                          s.max_angle_deg, **kw)
+
+
+def _engine_3d(s, storage="f32"):
+    from seisproc_b200.engine import MigrationEngine
+    eng = MigrationEngine(storage=storage)
+    return eng.migrate_bin_full(
+        traces=s.traces.cpu().numpy(), source_x=s.source_x, source_y=s.source_y,
+        receiver_x=s.receiver_x, receiver_y=s.receiver_y, origin_x=s.origin_x,
+        origin_y=s.origin_y, il_spacing=s.il_spacing, xl_spacing=s.xl_spacing, azimuth_deg=0.0,
+        n_il=s.n_il, n_xl=s.n_xl, dt_ms=s.dt_ms, t_min_ms=0.0, n_times=s.n_times,
+        max_aperture_m=s.max_aperture_m, max_angle_deg=s.max_angle_deg, normalize=False,
+        velocity_model=s.vrms)
+
+
+def test_vrms_3d_matches_fp64_oracle():
+    s = _small_3d()
+    img, fold = _engine_3d(s)
+    oi, of = _oracle_3d(s)
+    err = rel_l2(img.reshape(s.n_times, -1), oi)
+    flips = np.abs(fold.reshape(s.n_times, -1) - of).sum()
+    assert err <= FP32_TOL, err
+    assert flips <= max(2, FOLD_FLIP_FRAC * of.sum()), flips
+
+
+def test_utm_coordinates_float64_origin():
+    """World coordinates near (5e5, 6e6) m: FP64 origin subtraction keeps FP32 accuracy."""
+    s = _small_3d(utm=(5.0e5, 6.0e6))
+    img, fold = _engine_3d(s)
+    oi, of = _oracle_3d(s)
+    assert rel_l2(img.reshape(s.n_times, -1), oi) <= FP32_TOL
+
+
+@pytest.mark.parametrize("storage,tol", [("f16", 1e-3), ("bf16", 4e-3)])
+def test_16bit_storage_error_vs_fp64(storage, tol):
+    s = _small_3d(seed=4)
+    img, _ = _engine_3d(s, storage=storage)
+    oi, _ = _oracle_3d(s)
+    err = rel_l2(img.reshape(s.n_times, -1), oi)
+    assert err <= tol, f"{storage}: rel-L2 {err:.3e}"
+
+
+def test_deterministic_bitwise():
+    s = _small_3d(seed=5)
+    a, fa = _engine_3d(s)
+    b, fb = _engine_3d(s)
+    assert np.array_equal(a, b) and np.array_equal(fa, fb)
+
+
+def test_no_traces_gives_zero_image():
+    from seisproc_b200.engine import MigrationEngine
+    img, fold = MigrationEngine().migrate_bin_full(
+        traces=np.zeros((100, 0), np.float32), source_x=np.zeros(0), source_y=np.zeros(0),
+        receiver_x=np.zeros(0), receiver_y=np.zeros(0), origin_x=0, origin_y=0, il_spacing=25,
+        xl_spacing=25, azimuth_deg=0, n_il=3, n_xl=2, dt_ms=4, t_min_ms=0, normalize=False)
+    assert img.shape == (100, 3, 2) and not img.any() and not fold.any()
+
+
+def test_traces_outside_aperture_contribute_nothing():
+    from seisproc_b200.engine import MigrationEngine
+    n = 50
+    x = np.full(n, 1.0e5)
+    img, fold = MigrationEngine().migrate_bin_full(
+        traces=np.random.RandomState(0).randn(64, n).astype(np.float32), source_x=x,
+        source_y=x, receiver_x=x, receiver_y=x, origin_x=0, origin_y=0, il_spacing=25,
+        xl_spacing=25, azimuth_deg=0, n_il=4, n_xl=4, dt_ms=4, t_min_ms=0,
+        max_aperture_m=1000, normalize=False)
+    assert not img.any() and not fold.any()
+
+
+def test_invalid_velocity_rejected():
+    """A velocity that makes depth decrease with t0 is rejected by the device check."""
+    s = _small_3d(seed=6, n_traces=500, n_samples=64)
+    v = np.ascontiguousarray(s.vrms[::-1] * np.linspace(3, 1, s.n_times)[:, None, None],
+                             dtype=np.float32)
+    s.vrms = v
+    with pytest.raises(ValueError):
+        _engine_3d(s)
+
+
+def test_normalize_by_fold_kat():
+    """Known answers of the reference test (tests/test_kirchhoff_kernel.py:393-406)."""
+    from seisproc_b200.kirchhoff import normalize_by_fold
+    image = torch.tensor([[[10.0, 20.0], [30.0, 0.0]]])
+    fold = torch.tensor([[[2.0, 4.0], [3.0, 0.0]]])
+    n = normalize_by_fold(image, fold, min_fold=1)
+    assert torch.allclose(n, torch.tensor([[[5.0, 5.0], [10.0, 0.0]]]))
+    n2 = normalize_by_fold(torch.tensor([[[10.0, 20.0]]]), torch.tensor([[[1.0, 0.5]]]), 1)
+    assert n2[0, 0, 0].item() == 10.0 and n2[0, 0, 1].item() == 20.0

@@ -1,0 +1,204 @@
+"""The oracles, pinned against the reference's own outputs (golden fixtures
+generated by running it: tests/golden/make_golden.py) and against the
+known answers of the reference's tests."""
+import hashlib
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden_grid, load_golden, rel_l2
+from oracle import pstm_fp64 as O
+from oracle import ref_port as P
+
+
+def _golden_inputs(d):
+    g = golden_grid(d)
+    nt = int(d["n_times"])
+    il = np.arange(g["n_il"])[:, None]
+    xl = np.arange(g["n_xl"])[None, :]
+    cx = (g["origin_x"] + il * g["il_spacing"] + 0 * xl).ravel().astype(np.float32)
+    cy = (g["origin_y"] + 0 * il + xl * g["xl_spacing"]).ravel().astype(np.float32)
+    t_ms = (np.arange(nt, dtype=np.float32) * np.float32(g["dt_ms"]) +
+            np.float32(g["t_min_ms"])).astype(np.float64)
+    return g, nt, cx, cy, t_ms
+
+
+@pytest.mark.parametrize("name", ["full_2d_small", "full_2d_tda_tmin", "full_3d_mini"])
+def test_fp64_oracle_matches_reference(name):
+    d = load_golden(name)
+    g, nt, cx, cy, t_ms = _golden_inputs(d)
+    img, fold = O.migrate_fp64(d["traces"], d["source_x"], d["source_y"], d["receiver_x"],
+                               d["receiver_y"], cx, cy, t_ms, g["velocity_mps"], g["dt_ms"],
+                               g["t_min_ms"], g["max_aperture_m"], g["max_angle_deg"],
+                               time_dependent=bool(d["tda"]))
+    assert rel_l2(img, d["image"].reshape(nt, -1)) < 2e-5
+    assert np.array_equal(fold, d["fold"].reshape(nt, -1))
+
+
+@pytest.mark.parametrize("name", ["full_2d_small", "full_2d_tda_tmin", "full_3d_mini"])
+def test_port_is_bitexact_with_reference(name):
+    d = load_golden(name)
+    g = golden_grid(d)
+    img, fold = P.engine_full_port(d["traces"], d["source_x"], d["source_y"], d["receiver_x"],
+                                   d["receiver_y"], g["origin_x"], g["origin_y"],
+                                   g["il_spacing"], g["xl_spacing"], g["n_il"], g["n_xl"],
+                                   g["dt_ms"], g["t_min_ms"], int(d["n_times"]),
+                                   g["velocity_mps"], g["max_aperture_m"], g["max_angle_deg"],
+                                   bool(d["tda"]))
+    assert np.array_equal(img.numpy(), d["image"])
+    assert np.array_equal(fold.numpy(), d["fold"])
+
+
+def test_migrator_oracle_matches_reference():
+    """clamp='migrator' / weight='spreading' restate KirchhoffMigrator's direct branch."""
+    d = load_golden("migrator_mini")
+    ox, oy, dx, dy, nil, nxl, dt, tmin, v, A, ang, nt, gdt = d["grid"]
+    nil, nxl, nt = int(nil), int(nxl), int(nt)
+    il = np.arange(nil)[:, None]
+    xl = np.arange(nxl)[None, :]
+    cx = (np.float32(ox) + (il * np.float32(dx)).astype(np.float32) + 0 * xl).ravel()
+    cy = (np.float32(oy) + 0 * il + (xl * np.float32(dy)).astype(np.float32)).ravel()
+    t_ms = (np.arange(nt) * gdt).astype(np.float32).astype(np.float64) * 1000.0
+    img, fold = O.migrate_fp64(d["traces"], d["source_x"], d["source_y"], d["receiver_x"],
+                               d["receiver_y"], cx, cy, t_ms, v, dt, 0.0, A, ang,
+                               weight="spreading", clamp="migrator")
+    assert rel_l2(img, d["image"].reshape(nt, -1)) < 1e-4
+    assert np.abs(fold - d["fold"].reshape(nt, -1)).sum() <= 2
+
+
+def test_full_2d_config_port_matches_reference():
+    """The full-size 2D workload, regenerated from its seed (SHA-256 pinned)."""
+    from seisproc_b200 import synthetic
+    ref = load_golden("full_2d_config")
+    s = synthetic.survey_2d(seed=1234)
+    tr = s.traces.numpy()
+    assert hashlib.sha256(tr.astype(np.float32).tobytes()).hexdigest() == str(ref["input_sha256"])
+    torch.set_num_threads(4)
+    img, fold = P.engine_full_port(tr, s.source_x, s.source_y, s.receiver_x, s.receiver_y,
+                                   s.origin_x, s.origin_y, s.il_spacing, s.xl_spacing, s.n_il,
+                                   s.n_xl, s.dt_ms, s.t_min_ms, s.n_times, s.velocity_mps,
+                                   s.max_aperture_m, s.max_angle_deg)
+    assert np.array_equal(img.numpy(), ref["image"])
+    assert np.array_equal(fold.numpy(), ref["fold"])
+
+
+# --- known answers restated from the reference's tests -----------------------
+
+def _one_trace(h_s, h_r, z_m, v, n_s=2048, dt=1.0, weight="none", ramp=True):
+    """One trace with x[i] = i (linear interpolation is exact); source and
+    receiver at horizontal distances h_s, h_r (on opposite sides) from the
+    single output column; returns the oracle value at the sample where z = z_m."""
+    tr = (np.arange(n_s, dtype=np.float64) if ramp else np.ones(n_s))[:, None]
+    t0 = 2000.0 * z_m / v
+    t_ms = np.array([t0])
+    img, fold = O.migrate_fp64(tr, [-h_s], [0.0], [h_r], [0.0], [0.0], [0.0], t_ms, v, dt, 0.0,
+                               1e6, 89.9, weight=weight)
+    return img[0, 0], fold[0, 0]
+
+
+def test_kat_zero_offset_traveltime():
+    # tests/test_migration_core.py:72-80: z = 1000 m, v = 2000 -> one leg 0.5 s
+    val, fold = _one_trace(0.0, 0.0, 1000.0, 2000.0)
+    assert fold == 1 and val == pytest.approx(1000.0, rel=1e-9)  # 2 legs x 500 ms at 1 ms
+
+
+def test_kat_offset_traveltime():
+    # tests/test_migration_core.py:82-95: x = 750, z = 1000 -> r = 1250, 0.625 s per leg
+    val, _ = _one_trace(750.0, 750.0, 1000.0, 2000.0)
+    assert val == pytest.approx(1250.0, rel=1e-9)
+
+
+def test_kat_3d_offset_traveltime():
+    # tests/test_migration_core.py:97-110: (300, 400, 1200) -> r = 1300, 0.65 s per leg
+    tr = np.arange(4096, dtype=np.float64)[:, None]
+    img, _ = O.migrate_fp64(tr, [300.0], [400.0], [300.0], [400.0], [0.0], [0.0],
+                            np.array([1200.0]), 2000.0, 1.0, 0.0, 1e6, 89.9, weight="none")
+    assert img[0, 0] == pytest.approx(1300.0, rel=1e-9)
+
+
+def test_kat_angle_mask_45_degrees():
+    # tests/test_migration_core.py:158-166: h = z is exactly 45 degrees
+    tr = np.ones((4096, 1))
+    z, v = 1000.0, 2000.0
+    t_ms = np.array([2000.0 * z / v])
+    for h, expect in ((999.0, 1.0), (1001.0, 0.0)):
+        _, fold = O.migrate_fp64(tr, [h], [0.0], [h], [0.0], [0.0], [0.0], t_ms, v, 1.0, 0.0,
+                                 1e6, 45.0)
+        assert fold[0, 0] == expect
+
+
+def test_kat_interpolation_clamps():
+    # tests/test_kirchhoff_kernel.py:61-85: times beyond the trace read the last samples
+    tr = np.array([1.0, 2.0, 3.0, 4.0, 5.0])[:, None]
+    img, fold = O.migrate_fp64(tr, [0.0], [0.0], [0.0], [0.0], [0.0], [0.0], np.array([100.0]),
+                               2000.0, 2.0, 0.0, 1e6, 89.0, weight="none")
+    assert img[0, 0] == pytest.approx(4.999, abs=1e-9)  # clamp at n - 1.001
+
+
+def test_kat_spreading_ratio():
+    # tests/test_weights.py:368-379: doubling both distances quarters 1/(r_s r_r)
+    a, _ = _one_trace(0.0, 0.0, 500.0, 2000.0, n_s=8192, weight="spreading", ramp=False)
+    b, _ = _one_trace(0.0, 0.0, 1000.0, 2000.0, n_s=8192, weight="spreading", ramp=False)
+    assert a / b == pytest.approx(4.0, rel=1e-4)
+
+
+def test_normalize_by_fold_kat():
+    # tests/test_kirchhoff_kernel.py:393-406
+    img = np.array([[[10.0, 20.0], [30.0, 0.0]]])
+    fold = np.array([[[2.0, 4.0], [3.0, 0.0]]])
+    assert np.allclose(O.normalize_by_fold_fp64(img, fold, 1), [[[5, 5], [10, 0]]])
+    out = O.normalize_by_fold_fp64(np.array([[[10.0, 20.0]]]), np.array([[[1.0, 0.5]]]), 1)
+    assert out[0, 0, 0] == 10.0 and out[0, 0, 1] == 20.0
+
+
+# --- oracle self-consistency -------------------------------------------------
+
+def test_triangle_double_integral_equals_explicit_sum():
+    rs = np.random.RandomState(0)
+    tr = rs.randn(40)
+    i2 = O.double_integral(tr[None, :])[0]
+    i1_last = tr.sum()
+    for i in (0, 3, 17, 39):
+        for L in (1, 2, 5):
+            y = (O._i2_interp(i2, i1_last, np.array(i + L, float)) -
+                 2 * O._i2_interp(i2, i1_last, np.array(i, float)) +
+                 O._i2_interp(i2, i1_last, np.array(i - L, float))) / (L * L)
+            assert y == pytest.approx(O.triangle_explicit(tr, i, L), abs=1e-10)
+
+
+def test_oracle_adjoint_dot_product():
+    rs = np.random.RandomState(7)
+    n_s, n_tr, n_t = 64, 30, 40
+    sx, sy = rs.uniform(0, 300, n_tr), rs.uniform(0, 300, n_tr)
+    rx, ry = sx + rs.uniform(-100, 100, n_tr), sy + rs.uniform(-100, 100, n_tr)
+    cx, cy = np.array([100.0, 150.0, 200.0]), np.array([120.0, 150.0, 180.0])
+    t_ms = np.arange(n_t) * 4.0
+    d = rs.randn(n_s, n_tr)
+    m = rs.randn(n_t, 3)
+    Lt_d, _ = O.migrate_fp64(d, sx, sy, rx, ry, cx, cy, t_ms, 1800.0, 4.0, 0.0, 250.0, 60.0)
+    L_m = O.demigrate_fp64(m, n_s, sx, sy, rx, ry, cx, cy, t_ms, 1800.0, 4.0, 0.0, 250.0, 60.0)
+    a = float(np.sum(L_m * d))
+    b = float(np.sum(m * Lt_d))
+    assert abs(a - b) <= 1e-12 * max(abs(a), abs(b))
+
+
+def test_oracle_vgrad_matches_finite_difference():
+    rs = np.random.RandomState(3)
+    n_s, n_tr, n_t = 200, 40, 60
+    sx, sy = rs.uniform(0, 400, n_tr), rs.uniform(0, 400, n_tr)
+    rx, ry = rs.uniform(0, 400, n_tr), rs.uniform(0, 400, n_tr)
+    cx, cy = np.array([200.0]), np.array([200.0])
+    t_ms = 100.0 + np.arange(n_t) * 4.0
+    tt = np.arange(n_s) * 4.0e-3
+    d = np.sin(2 * np.pi * 12 * tt)[:, None] * rs.uniform(0.5, 1.5, n_tr)[None, :]
+    v = 1800.0 + 2.0 * np.arange(n_t)[:, None]
+    g = rs.randn(n_t, 1)
+    gv = O.vgrad_fp64(d, g, sx, sy, rx, ry, cx, cy, t_ms, v, 4.0, 0.0, 1e5, 89.0)
+    dv = rs.randn(n_t, 1)
+    eps = 1e-3
+    f = lambda vv: float(np.sum(g * O.migrate_fp64(d, sx, sy, rx, ry, cx, cy, t_ms, vv, 4.0,
+                                                   0.0, 1e5, 89.0)[0]))
+    fd = (f(v + eps * dv) - f(v - eps * dv)) / (2 * eps)
+    assert float(np.sum(gv * dv)) == pytest.approx(fd, rel=2e-3)
