@@ -295,6 +295,10 @@ __global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather_kernel(const KA
     }
 
     if (col_ok) {
+      // One straight-line sweep over all M groups per trace (no branch between
+      // groups, so the compiler can interleave their MUFU/LDS chains).  Traces
+      // whose first contributing sample lies inside this warp's range take the
+      // masked sweep; samples before k_start get weight 0.
       for (int t = 0; t < cnt; ++t) {
         const float4 su = setup[cl * B + t];
         const int ks = __float_as_int(su.z);
@@ -303,71 +307,77 @@ __global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather_kernel(const KA
             (OP == OP_ADJ ? smem_addr(tacc + t * E) - (kMagicBits << 2)
                           : smem_addr(exps + t * E) - (kMagicBits << 3));
         const f2 hs2b = f2_bcast(su.x), hr2b = f2_bcast(su.y);
+        auto sweep = [&](auto masked_tag) {
+          constexpr bool MASKED = decltype(masked_tag)::value;
 #pragma unroll
-        for (int i = 0; i < M; ++i) {
-          const int kc = kw + 64 * i;
-          if (kc + 64 <= ks) continue;
-          const f2 rrs = f2_add(hs2b, zz[i]);
-          const f2 rrr = f2_add(hr2b, zz[i]);
-          const f2 qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
-          const f2 qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
-          const f2 sum = f2_fma(rrr, qr, f2_mul(rrs, qs));
-          f2 id = f2_fma(sum, aa[i], bb);
-          const f2 id_raw = id;
-          id.x = fminf(id.x, hi_c);
-          id.y = fminf(id.y, hi_c);
-          if (LOWCLAMP) {
-            id.x = fmaxf(id.x, lo_c);
-            id.y = fmaxf(id.y, lo_c);
+          for (int i = 0; i < M; ++i) {
+            const f2 rrs = f2_add(hs2b, zz[i]);
+            const f2 rrr = f2_add(hr2b, zz[i]);
+            const f2 qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
+            const f2 qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
+            const f2 sum = f2_fma(rrr, qr, f2_mul(rrs, qs));
+            f2 id = f2_fma(sum, aa[i], bb);
+            const f2 id_raw = id;
+            id.x = fminf(id.x, hi_c);
+            id.y = fminf(id.y, hi_c);
+            if (LOWCLAMP) {
+              id.x = fmaxf(id.x, lo_c);
+              id.y = fmaxf(id.y, lo_c);
+            }
+            const f2 tm = f2_add_rm(id, magic2);
+            const f2 fr = f2_sub(id, f2_sub(tm, magic2));
+            const f2 p = f2_mul(qs, qr);
+            f2 w;  // weight without the per-sample z^2 factor
+            if (WM == W_OBL_SPREAD) {
+              w = f2_mul(p, p);
+            } else if (WM == W_OBL) {
+              w = p;
+            } else if (WM == W_SPREAD) {
+              w = f2{p.x * rcp_approx(fmaf(1e-6f, p.x, 1.0f)),
+                     p.y * rcp_approx(fmaf(1e-6f, p.y, 1.0f))};
+            } else {
+              w = f2{1.0f, 1.0f};
+            }
+            if constexpr (MASKED) {
+              const int klo = kw + 64 * i + lane;
+              w.x = klo >= ks ? w.x : 0.f;
+              w.y = klo + 32 >= ks ? w.y : 0.f;
+            }
+            if (OP == OP_FWD) {
+              const f2 e0 = lds_f2(ebase + (__float_as_uint(tm.x) << 3));
+              const f2 e1 = lds_f2(ebase + (__float_as_uint(tm.y) << 3));
+              const f2 amp = f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
+              acc[i] = f2_fma(amp, w, acc[i]);
+            } else if (OP == OP_ADJ) {
+              const f2 g = f2_mul(acc[i], w);
+              const uint32_t a0 = ebase + (__float_as_uint(tm.x) << 2);
+              const uint32_t a1 = ebase + (__float_as_uint(tm.y) << 2);
+              const float g0 = g.x * fr.x, g1 = g.y * fr.y;
+              asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a0), "f"(g.x - g0) : "memory");
+              asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a0 + 4), "f"(g0) : "memory");
+              asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a1), "f"(g.y - g1) : "memory");
+              asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a1 + 4), "f"(g1) : "memory");
+            } else {  // OP_VGRAD (obliquity x spreading)
+              const f2 e0 = lds_f2(ebase + (__float_as_uint(tm.x) << 3));
+              const f2 e1 = lds_f2(ebase + (__float_as_uint(tm.y) << 3));
+              const f2 amp = f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
+              // slope of the interpolant in samples; zero where the index is clamped
+              const f2 slope = f2{(id_raw.x < hi_c && id_raw.x > lo_c) ? e0.y : 0.f,
+                                  (id_raw.y < hi_c && id_raw.y > lo_c) ? e1.y : 0.f};
+              const f2 q2 = f2_fma(qs, qs, f2_mul(qr, qr));
+              const f2 one_m = f2_sub(f2_bcast(1.0f), f2_mul(zz[i], q2));
+              const f2 hq = f2_fma(hs2b, qs, f2_mul(hr2b, qr));
+              // 2 amp (1 - z^2 (qs^2 + qr^2)) - slope a (hs^2 qs + hr^2 qr)
+              const f2 term = f2_sub(f2_mul(f2_bcast(2.0f), f2_mul(amp, one_m)),
+                                     f2_mul(f2_mul(slope, aa[i]), hq));
+              acc[i] = f2_fma(term, w, acc[i]);
+            }
           }
-          const f2 tm = f2_add_rm(id, magic2);
-          const f2 fr = f2_sub(id, f2_sub(tm, magic2));
-          const f2 p = f2_mul(qs, qr);
-          f2 w;  // weight without the per-sample z^2 factor
-          if (WM == W_OBL_SPREAD) {
-            w = f2_mul(p, p);
-          } else if (WM == W_OBL) {
-            w = p;
-          } else if (WM == W_SPREAD) {
-            w = f2{p.x * rcp_approx(fmaf(1e-6f, p.x, 1.0f)), p.y * rcp_approx(fmaf(1e-6f, p.y, 1.0f))};
-          } else {
-            w = f2{1.0f, 1.0f};
-          }
-          if (kc < ks) {  // partial group: mask samples before k_start
-            const int klo = kc + lane;
-            if (klo < ks) w.x = 0.f;
-            if (klo + 32 < ks) w.y = 0.f;
-          }
-          if (OP == OP_FWD) {
-            const f2 e0 = lds_f2(ebase + (__float_as_uint(tm.x) << 3));
-            const f2 e1 = lds_f2(ebase + (__float_as_uint(tm.y) << 3));
-            const f2 amp = f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
-            acc[i] = f2_fma(amp, w, acc[i]);
-          } else if (OP == OP_ADJ) {
-            const f2 g = f2_mul(acc[i], w);
-            const uint32_t a0 = ebase + (__float_as_uint(tm.x) << 2);
-            const uint32_t a1 = ebase + (__float_as_uint(tm.y) << 2);
-            const float g0 = g.x * fr.x, g1 = g.y * fr.y;
-            asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a0), "f"(g.x - g0) : "memory");
-            asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a0 + 4), "f"(g0) : "memory");
-            asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a1), "f"(g.y - g1) : "memory");
-            asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a1 + 4), "f"(g1) : "memory");
-          } else {  // OP_VGRAD (obliquity x spreading)
-            const f2 e0 = lds_f2(ebase + (__float_as_uint(tm.x) << 3));
-            const f2 e1 = lds_f2(ebase + (__float_as_uint(tm.y) << 3));
-            const f2 amp = f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
-            // slope of the interpolant in samples; zero where the index is clamped
-            const f2 slope = f2{(id_raw.x < hi_c && id_raw.x > lo_c) ? e0.y : 0.f,
-                                (id_raw.y < hi_c && id_raw.y > lo_c) ? e1.y : 0.f};
-            const f2 q2 = f2_fma(qs, qs, f2_mul(qr, qr));
-            const f2 one_m = f2_sub(f2_bcast(1.0f), f2_mul(zz[i], q2));
-            const f2 hq = f2_fma(hs2b, qs, f2_mul(hr2b, qr));
-            // 2 amp (1 - z^2 (qs^2 + qr^2)) - slope a (hs^2 qs + hr^2 qr)
-            const f2 term = f2_sub(f2_mul(f2_bcast(2.0f), f2_mul(amp, one_m)),
-                                   f2_mul(f2_mul(slope, aa[i]), hq));
-            acc[i] = f2_fma(term, w, acc[i]);
-          }
-        }
+        };
+        if (ks <= kw)
+          sweep(std::false_type{});
+        else
+          sweep(std::true_type{});
       }
     }
     __syncthreads();

@@ -1,0 +1,106 @@
+"""BaseMigrator drop-in on the GPU: KirchhoffMigrator (direct DSR branch) against
+the reference's own output, accumulation semantics, migrate_dataset
+normalisation, and the kernel known answers through the C ABI."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _mig_from_golden(d, **kw):
+    from seisproc_b200 import models as M
+    from seisproc_b200.migrator import KirchhoffMigrator
+    ox, oy, dx, dy, nil, nxl, dt, tmin, v, A, ang, nt, gdt = d["grid"]
+    grid = M.OutputGrid(n_time=int(nt), n_inline=int(nil), n_xline=int(nxl), dt=float(gdt),
+                        d_inline=float(dx), d_xline=float(dy), t0=0.0, x_origin=float(ox),
+                        y_origin=float(oy))
+    cfg = M.MigrationConfig(output_grid=grid, max_aperture_m=float(A), max_angle_deg=float(ang),
+                            **kw)
+    mig = KirchhoffMigrator(M.create_constant_velocity(float(v)), cfg, use_traveltime_lut=False)
+    gather = M.SeismicData(traces=d["traces"], sample_rate=float(dt))
+    geom = M.MigrationGeometry(d["source_x"], d["source_y"], d["receiver_x"], d["receiver_y"])
+    return mig, gather, geom
+
+
+def test_kirchhoff_migrator_matches_reference():
+    d = load_golden("migrator_mini")
+    mig, gather, geom = _mig_from_golden(d)
+    img, fold = mig.migrate_gather(gather, geom)
+    assert rel_l2(img.cpu().numpy(), d["image"]) <= 1e-4
+    assert np.abs(fold.cpu().numpy() - d["fold"]).sum() <= 2
+
+
+def test_migrate_gather_accumulates():
+    d = load_golden("migrator_mini")
+    mig, gather, geom = _mig_from_golden(d)
+    a, fa = mig.migrate_gather(gather, geom)
+    a2, fa2 = mig.migrate_gather(gather, geom, a.clone(), fa.clone())
+    assert torch.allclose(a2, 2 * a, rtol=1e-6, atol=0) and torch.equal(fa2, 2 * fa)
+
+
+def test_migrate_dataset_normalises_and_mutes():
+    d = load_golden("migrator_mini")
+    mig, gather, geom = _mig_from_golden(d, min_fold=3)
+    res = mig.migrate_dataset([gather, gather], [geom, geom])
+    img, fold = mig.migrate_gather(gather, geom)
+    img, fold = 2 * img.cpu().numpy(), 2 * fold.cpu().numpy()
+    expect = np.where(fold >= 3, img / np.maximum(fold, 3), 0.0)
+    assert rel_l2(res.image, expect) <= 1e-6
+    assert res.fold.dtype == np.int32 and np.array_equal(res.fold, fold.astype(np.int32))
+
+
+def test_offset_selection():
+    d = load_golden("migrator_mini")
+    mig, gather, geom = _mig_from_golden(d, min_offset_m=100.0, max_offset_m=300.0)
+    img, fold = mig.migrate_gather(gather, geom)
+    off = geom.offset
+    keep = (off >= 100.0) & (off <= 300.0)
+    from seisproc_b200 import models as M
+    mig2, _, _ = _mig_from_golden(d)
+    g2 = M.SeismicData(traces=np.ascontiguousarray(d["traces"][:, keep]), sample_rate=4.0)
+    geo2 = M.MigrationGeometry(d["source_x"][keep], d["source_y"][keep], d["receiver_x"][keep],
+                               d["receiver_y"][keep])
+    img2, fold2 = mig2.migrate_gather(g2, geo2)
+    assert torch.equal(fold, fold2) and torch.allclose(img, img2)
+
+
+def _plan_one_trace(h_s, h_r, weight="none", data=None, n_s=4096, v=2000.0, n_t=400,
+                    dt_out=4.0, dt_in=1.0, angle=89.9):
+    from seisproc_b200.kirchhoff import PSTMPlan
+    dev = torch.device("cuda")
+    f64 = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    plan = PSTMPlan(f64([-h_s]), f64([0.0]), f64([h_r]), f64([0.0]), n_il=1, n_xl=1,
+                    n_times=n_t, origin_x=0.0, origin_y=0.0, il_dx=25.0, il_dy=0.0, xl_dx=0.0,
+                    xl_dy=25.0, t0_ms=0.0, dt_ms=dt_out, n_samples=n_s, in_t0_ms=0.0,
+                    in_dt_ms=dt_in, max_aperture_m=1e6, max_angle_deg=angle, weight=weight)
+    tr = torch.arange(n_s, dtype=torch.float32) if data is None else data
+    img, fold = plan.migrate(tr.view(n_s, 1).to(dev), torch.tensor([v]))
+    plan.check()
+    plan.close()
+    return img.view(-1).cpu().numpy(), fold.view(-1).cpu().numpy()
+
+
+def test_kernel_kat_traveltimes():
+    """x[i] = i makes the migrated value the sample index itself: t = (r_s + r_r)/V
+    (tests/test_migration_core.py:72-110 restated through the kernel)."""
+    img, fold = _plan_one_trace(750.0, 750.0, angle=60.0)
+    # output sample k: t0 = 4k ms, z = V t0 / 2 = 4k m; idx = 2 sqrt(750^2 + z^2) / V ms / 1 ms
+    k = np.arange(400)
+    z = 2000.0 * (4.0 * k / 1000.0) / 2.0
+    expect = 2.0 * np.sqrt(750.0 ** 2 + z ** 2) / 2000.0 * 1000.0
+    valid = fold > 0
+    # 60 degrees: h < tan(60) z  <=>  750 < 1.732 * 4k  <=>  k >= 109
+    assert valid[109] and not valid[108] and valid.sum() == 400 - 109
+    assert np.allclose(img[valid], np.minimum(expect[valid], 4096 - 1.001), rtol=2e-6)
+    assert img[250] == pytest.approx(2.0 * 1250.0 / 2000.0 * 1000.0, rel=2e-6)  # z=1000: 0.625 s/leg
+
+
+def test_kernel_kat_spreading_ratio():
+    """tests/test_weights.py:368-379: doubling r quarters 1/(r_s r_r)."""
+    img, _ = _plan_one_trace(0.0, 0.0, weight="spreading",
+                             data=torch.ones(4096, dtype=torch.float32))
+    # z = 4k m at sample k: r = 4k, w = 1 / (16 k^2 + 1e-6)
+    assert img[125] / img[250] == pytest.approx(4.0, rel=1e-5)
