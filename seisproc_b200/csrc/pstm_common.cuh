@@ -10,10 +10,9 @@
 #define PSTM_ERR_BOUNDS 2
 #define PSTM_ERR_VELOCITY 4
 
-// Bounded spin on an mbarrier: ~2^26 polls of try_wait (each poll itself
-// suspends for a hardware-defined interval) is several seconds, far beyond any
-// legitimate wait for one bulk copy.
-#define PSTM_SPIN_LIMIT (1u << 26)
+// Bounded waits on an mbarrier give up after this many nanoseconds of the
+// global timer (2 s: far beyond any legitimate wait for one pipeline stage).
+#define PSTM_WAIT_NS 2000000000ull
 
 namespace pstm {
 
@@ -100,9 +99,15 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
 }
 // Returns true when the phase with parity `parity` has completed, false if the
 // bounded spin ran out.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t addr = smem_addr(bar);
-  for (uint32_t it = 0; it < PSTM_SPIN_LIMIT; ++it) {
+  const uint32_t addr = smem_addr(bar);
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -112,8 +117,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((it & 63) == 0) {
+      const uint64_t now = global_ns();
+      if (it == 0)
+        t0 = now;
+      else if (now - t0 > PSTM_WAIT_NS)
+        return false;
+    }
   }
-  return false;
 }
 
 // 1-D bulk copy global -> shared (TMA engine), completion signalled on `bar`.

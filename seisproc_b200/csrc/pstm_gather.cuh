@@ -32,6 +32,7 @@ struct KArgs {
   const float* in_img;
   float* accum;
   int* err;
+  int ring_stages, ring_rows;  // pipelined kernel: stages x rows per stage
 };
 
 __device__ __forceinline__ float vel_at(const KArgs& A, int k, int c) {

@@ -1,0 +1,408 @@
+// Warp-specialised gather kernel (forward migration and V-gradient).
+//
+// CTA = NW consumer warps + 1 producer warp.  The producer streams the rows of
+// the tile's trace list through an NSTAGE-deep ring of shared-memory stages
+// (kBlockTraces rows each) with 1-D TMA bulk copies; `full[s]` completes on the
+// copies' byte count, `empty[s]` when every consumer warp has finished the
+// stage.  Consumer warps never synchronise with each other: each one computes
+// the per-(column, trace) set-up for 32 list entries at a time (one lane per
+// trace: leg distances and the first contributing sample by binary search in
+// the CTA's threshold table), then sweeps the traces, taking each trace's
+// set-up from its lane by shuffle.  Samples are read straight from the staged
+// row: two shared loads (x[i0], x[i0+1]) and one f32x2 FMA per sample pair.
+#pragma once
+#include "pstm_gather.cuh"
+
+namespace pstm {
+
+constexpr int kMaxStages = 4;
+constexpr int kSmemBudget = 227 * 1024;
+
+struct Smem2 {
+  int bars, thr, raw, total;
+};
+// Ring of `stages` stages of `sb` trace rows each.
+__host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, int stages, int sb) {
+  Smem2 L;
+  int o = 0;
+  L.bars = o;
+  o += 2 * kMaxStages * 8 + 16;
+  o = (o + 15) & ~15;
+  L.thr = o;
+  o += cols * T * 4;
+  o = (o + 127) & ~127;
+  L.raw = o;
+  o += stages * sb * S * elt;
+  L.total = o;
+  return L;
+}
+
+// Largest ring (up to 4 stages x 8 rows, at least 2 stages) that fits.
+inline bool ring_shape(int cols, int T, int S, int elt, int* stages, int* sb) {
+  for (int b = kBlockTraces; b >= 1; b >>= 1)
+    for (int st = kMaxStages; st >= 2; --st)
+      if (smem2_layout(cols, T, S, elt, st, b).total <= kSmemBudget) {
+        *stages = st;
+        *sb = b;
+        return true;
+      }
+  return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+template <typename ST>
+__device__ __forceinline__ float lds_elem(uint32_t addr);
+template <>
+__device__ __forceinline__ float lds_elem<float>(uint32_t addr) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
+template <>
+__device__ __forceinline__ float lds_elem<__nv_bfloat16>(uint32_t addr) {
+  unsigned short h;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=h"(h) : "r"(addr));
+  return __uint_as_float(((uint32_t)h) << 16);
+}
+template <>
+__device__ __forceinline__ float lds_elem<__half>(uint32_t addr) {
+  unsigned short h;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=h"(h) : "r"(addr));
+  return __half2float(__ushort_as_half(h));
+}
+
+template <int COLS, int WPC, int M, typename ST, int WM, int OP>
+__global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(const KArgs A) {
+  constexpr int NW = COLS * WPC;
+  constexpr int T = WPC * 64 * M;
+  constexpr int ES = (int)sizeof(ST);
+  constexpr int SHIFT = ES == 4 ? 2 : 1;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int S = A.S;
+  const int B = A.ring_rows, kStages = A.ring_stages;
+  const Smem2 L = smem2_layout(COLS, T, S, ES, kStages, B);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);
+  uint64_t* empty = full + kMaxStages;
+  int* abort_flag = reinterpret_cast<int*>(empty + kMaxStages);
+  float* thr = reinterpret_cast<float*>(smem + L.thr);
+  ST* raw = reinterpret_cast<ST*>(smem + L.raw);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int tile = blockIdx.x;
+  const int k0 = blockIdx.y * T;
+  const int kend = min(k0 + T, A.n_times);
+  const int nk = kend - k0;
+  const int n_c = A.n_il * A.n_xl;
+  const int64_t off0 = A.off[tile];
+  const int n_list = (int)(A.off[tile + 1] - off0);
+  const int nb = (n_list + B - 1) / B;
+  const int lo = window_lo(A, k0, Storage<ST>::kAlign);
+  const int rowlen = S - lo;
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, NW);
+    }
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  for (int e = tid; e < COLS * T; e += blockDim.x) {
+    const int q = e / T, kk = e - q * T;
+    int qil, qxl;
+    float v = -1.0f;
+    if (kk < nk && tile_column(A, tile, q, qil, qxl)) v = threshold(A, qil * A.n_xl + qxl, k0 + kk);
+    thr[e] = v;
+  }
+  __syncthreads();
+
+  if (warp == NW) {
+    // ------------------------------------------------------------ producer
+    const uint32_t bytes = (uint32_t)(rowlen * ES);
+    const ST* src = reinterpret_cast<const ST*>(A.traces);
+    for (int b = 0; b < nb; ++b) {
+      const int s = b % kStages;
+      if (b >= kStages) {
+        bool ok = true;
+        if (lane == 0) ok = mbar_wait(empty + s, ((b / kStages) - 1) & 1);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        if (!ok || *reinterpret_cast<volatile int*>(abort_flag)) {
+          if (lane == 0) {
+            set_error(A.err, PSTM_ERR_TIMEOUT);
+            *abort_flag = 1;
+          }
+          break;
+        }
+      }
+      const int cnt = min(B, n_list - b * B);
+      if (lane == 0) mbar_arrive_expect_tx(full + s, bytes * cnt);
+      __syncwarp();
+      if (lane < cnt) {
+        const int jj = A.list[off0 + (int64_t)b * B + lane];
+        bulk_g2s(raw + (s * B + lane) * S, src + (int64_t)jj * S + lo, bytes, full + s);
+      }
+    }
+    // keep the CTA (and its shared memory) alive until the copies in flight land
+    if (lane == 0) {
+      for (int b = max(0, nb - kStages); b < nb; ++b) mbar_wait(full + b % kStages, (b / kStages) & 1);
+    }
+    return;
+  }
+
+  // -------------------------------------------------------------- consumers
+  const int cl = warp / WPC, ts = warp % WPC;
+  int il, xl;
+  const bool col_ok = tile_column(A, tile, cl, il, xl);
+  const int c = col_ok ? il * A.n_xl + xl : 0;
+  float xc = 0.f, yc = 0.f;
+  if (col_ok) column_xy(A, il, xl, xc, yc);
+  const int kw = k0 + ts * 64 * M;
+  const bool warp_live = col_ok && kw < A.n_times;
+
+  f2 zz[M], aa[M], acc[M];
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const int kl = min(kw + 64 * i + lane, A.n_times - 1), kh = min(kl + 32, A.n_times - 1);
+    const float vl = vel_at(A, kl, c), vh = vel_at(A, kh, c);
+    const float zl = depth_of(vl, out_time_ms(kl, A.out_dt, A.out_t0));
+    const float zh = depth_of(vh, out_time_ms(kh, A.out_dt, A.out_t0));
+    zz[i] = f2{fmaf(zl, zl, kRadicandFloor), fmaf(zh, zh, kRadicandFloor)};
+    aa[i] = f2{1000.0f / (vl * A.in_dt), 1000.0f / (vh * A.in_dt)};
+    acc[i] = f2{0.f, 0.f};
+  }
+  const float bconst = -A.in_t0 / A.in_dt - (float)lo;
+  const f2 bb = f2_bcast(bconst);
+  const float hi_c = A.clamp_hi - (float)lo;
+  const float lo_c = -(float)lo;  // idx >= 0
+  // the lower clamp matters only where idx can reach 0: the first window, or
+  // output times before the first input sample
+  const bool lowclamp = (k0 == 0) || (A.out_t0 < A.in_t0);
+  const f2 magic2 = f2_bcast(kMagic);
+  const float* thr_c = thr + cl * T;
+  const uint32_t raw_base = smem_addr(raw) - (kMagicBits << SHIFT);
+  float sc = 1.0f;
+
+  bool aborted = false;
+  int slot = 0, stage = 0;
+  uint32_t phase = 0;
+  // the next chunk's list entries and geometry are fetched while the current
+  // chunk computes
+  int jj_next = (lane < n_list) ? A.list[off0 + lane] : 0;
+  float4 g_next = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (warp_live && lane < n_list) g_next = __ldg(A.geo + jj_next);
+  for (int p0 = 0; p0 < n_list && !aborted; p0 += 32) {
+    // set-up of 32 list entries, one per lane
+    float hs2 = 0.f, hr2 = 0.f;
+    int ks = warp_live ? kend : 0x7fffffff;  // kend: no contribution in this window
+    float tsc = 1.0f;
+    const int jj = jj_next;
+    if (p0 + lane < n_list) {
+      if (warp_live) {
+        leg_h2(xc, yc, g_next, hs2, hr2);
+        ks = k0 + first_valid(thr_c, nk, sqrtf(fmaxf(hs2, hr2)));
+      }
+      if (A.scales) tsc = __ldg(A.scales + jj);
+    }
+    const int pn = p0 + 32 + lane;
+    if (pn < n_list) jj_next = A.list[off0 + pn];
+    const int nt = min(32, n_list - p0);
+    for (int t = 0; t < nt; ++t) {
+      const int p = p0 + t;
+      if (t == 4 && warp_live && pn < n_list) g_next = __ldg(A.geo + jj_next);
+      if (slot == 0) {
+        bool ok = true;
+        if (lane == 0) ok = mbar_wait(full + stage, phase);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        if (!ok) {
+          if (lane == 0) {
+            set_error(A.err, PSTM_ERR_TIMEOUT);
+            *abort_flag = 1;
+          }
+          aborted = true;
+          break;
+        }
+      }
+      const int kst = __shfl_sync(0xffffffffu, ks, t);
+      if (kst < kw + 64 * M) {
+        const f2 hs2b = f2_bcast(__shfl_sync(0xffffffffu, hs2, t));
+        const f2 hr2b = f2_bcast(__shfl_sync(0xffffffffu, hr2, t));
+        if (std::is_same<ST, __half>::value) sc = __shfl_sync(0xffffffffu, tsc, t);
+        const uint32_t rbase = raw_base + (uint32_t)((stage * B + slot) * S * ES);
+        auto sweep = [&](auto masked_tag, auto low_tag) {
+          constexpr bool MASKED = decltype(masked_tag)::value;
+          constexpr bool LOWC = decltype(low_tag)::value;
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            const f2 rrs = f2_add(hs2b, zz[i]);
+            const f2 rrr = f2_add(hr2b, zz[i]);
+            const f2 qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
+            const f2 qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
+            const f2 sum = f2_fma(rrr, qr, f2_mul(rrs, qs));
+            f2 id = f2_fma(sum, aa[i], bb);
+            const f2 id_raw = id;
+            id.x = fminf(id.x, hi_c);
+            id.y = fminf(id.y, hi_c);
+            if constexpr (LOWC) {
+              id.x = fmaxf(id.x, lo_c);
+              id.y = fmaxf(id.y, lo_c);
+            }
+            const f2 tm = f2_add_rm(id, magic2);
+            const f2 fr = f2_sub(id, f2_sub(tm, magic2));
+            const uint32_t a0 = rbase + (__float_as_uint(tm.x) << SHIFT);
+            const uint32_t a1 = rbase + (__float_as_uint(tm.y) << SHIFT);
+            const f2 x0 = f2{lds_elem<ST>(a0), lds_elem<ST>(a1)};
+            const f2 x1 = f2{lds_elem<ST>(a0 + ES), lds_elem<ST>(a1 + ES)};
+            const f2 dx = f2_sub(x1, x0);
+            const f2 amp = f2_fma(fr, dx, x0);
+            const f2 p = f2_mul(qs, qr);
+            f2 w;
+            if (WM == W_OBL_SPREAD) {
+              w = f2_mul(p, p);
+            } else if (WM == W_OBL) {
+              w = p;
+            } else if (WM == W_SPREAD) {
+              w = f2{p.x * rcp_approx(fmaf(1e-6f, p.x, 1.0f)),
+                     p.y * rcp_approx(fmaf(1e-6f, p.y, 1.0f))};
+            } else {
+              w = f2{1.0f, 1.0f};
+            }
+            if (std::is_same<ST, __half>::value) w = f2_mul(w, f2_bcast(sc));
+            if constexpr (MASKED) {
+              const int klo = kw + 64 * i + lane;
+              w.x = klo >= kst ? w.x : 0.f;
+              w.y = klo + 32 >= kst ? w.y : 0.f;
+            }
+            if (OP == OP_FWD) {
+              acc[i] = f2_fma(amp, w, acc[i]);
+            } else {  // OP_VGRAD
+              const f2 slope = f2{(id_raw.x < hi_c && id_raw.x > lo_c) ? dx.x : 0.f,
+                                  (id_raw.y < hi_c && id_raw.y > lo_c) ? dx.y : 0.f};
+              const f2 q2 = f2_fma(qs, qs, f2_mul(qr, qr));
+              const f2 one_m = f2_sub(f2_bcast(1.0f), f2_mul(zz[i], q2));
+              const f2 hq = f2_fma(hs2b, qs, f2_mul(hr2b, qr));
+              const f2 term = f2_sub(f2_mul(f2_bcast(2.0f), f2_mul(amp, one_m)),
+                                     f2_mul(f2_mul(slope, aa[i]), hq));
+              acc[i] = f2_fma(term, w, acc[i]);
+            }
+          }
+        };
+        const bool masked = kst > kw;
+        if (lowclamp) {
+          if (masked)
+            sweep(std::true_type{}, std::true_type{});
+          else
+            sweep(std::false_type{}, std::true_type{});
+        } else {
+          if (masked)
+            sweep(std::true_type{}, std::false_type{});
+          else
+            sweep(std::false_type{}, std::false_type{});
+        }
+      }
+      if (++slot == B || p == n_list - 1) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty + stage);
+        slot = 0;
+        if (++stage == kStages) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+    }
+  }
+  if (aborted || !warp_live) return;
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const int klo = kw + 64 * i + lane, khi = klo + 32;
+    float fl = 1.f, fh = 1.f;
+    if (WM == W_OBL_SPREAD || WM == W_OBL || OP == OP_VGRAD) {
+      const int kl = min(klo, A.n_times - 1), kh = min(khi, A.n_times - 1);
+      const float vl = vel_at(A, kl, c), vh = vel_at(A, kh, c);
+      const float zl = depth_of(vl, out_time_ms(kl, A.out_dt, A.out_t0));
+      const float zh = depth_of(vh, out_time_ms(kh, A.out_dt, A.out_t0));
+      fl = zl * zl;
+      fh = zh * zh;
+      if (OP == OP_VGRAD) {
+        fl = klo < A.n_times ? fl / vl * A.in_img[(long long)klo * n_c + c] : 0.f;
+        fh = khi < A.n_times ? fh / vh * A.in_img[(long long)khi * n_c + c] : 0.f;
+      }
+    }
+    if (klo < A.n_times) A.out[(long long)klo * n_c + c] = acc[i].x * fl;
+    if (khi < A.n_times) A.out[(long long)khi * n_c + c] = acc[i].y * fh;
+  }
+}
+
+template <int COLS, int WPC, int M, typename ST, int WM, int OP>
+inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
+  auto kern = pstm_gather2_kernel<COLS, WPC, M, ST, WM, OP>;
+  const int T = WPC * 64 * M;
+  KArgs A2 = A;
+  if (!ring_shape(COLS, T, p->row_stride, (int)sizeof(ST), &A2.ring_stages, &A2.ring_rows))
+    return cudaErrorInvalidValue;
+  const Smem2 L = smem2_layout(COLS, T, p->row_stride, (int)sizeof(ST), A2.ring_stages,
+                               A2.ring_rows);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)p->n_tiles, (unsigned)((p->grid.n_times + T - 1) / T));
+  kern<<<grid, COLS * WPC * 32 + 32, L.total, s>>>(A2);
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <int COLS, int WPC, int M, typename ST, int OP>
+inline cudaError_t dispatch2_wm(const Plan* p, const KArgs& A, cudaStream_t s) {
+  const int wm = p->params.weight;
+  if constexpr (OP == OP_VGRAD || !std::is_same<ST, float>::value) {
+    if (wm != W_OBL_SPREAD) return cudaErrorNotSupported;
+    return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP>(p, A, s);
+  } else {
+    switch (wm) {
+      case W_OBL_SPREAD:
+        return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP>(p, A, s);
+      case W_SPREAD:
+        return launch2_one<COLS, WPC, M, ST, W_SPREAD, OP>(p, A, s);
+      case W_OBL:
+        return launch2_one<COLS, WPC, M, ST, W_OBL, OP>(p, A, s);
+      case W_NONE:
+        return launch2_one<COLS, WPC, M, ST, W_NONE, OP>(p, A, s);
+    }
+    return cudaErrorInvalidValue;
+  }
+}
+
+template <int COLS, int WPC, int M, int OP>
+inline cudaError_t dispatch2_st(const Plan* p, const KArgs& A, cudaStream_t s) {
+  switch (p->params.storage) {
+    case PSTM_F32:
+      return dispatch2_wm<COLS, WPC, M, float, OP>(p, A, s);
+    case PSTM_BF16:
+      return dispatch2_wm<COLS, WPC, M, __nv_bfloat16, OP>(p, A, s);
+    case PSTM_F16:
+      return dispatch2_wm<COLS, WPC, M, __half, OP>(p, A, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int OP>
+inline cudaError_t dispatch2_shape(const Plan* p, const KArgs& A, cudaStream_t s) {
+  switch (p->shape.id) {
+    case 1:
+    case 5:
+      return dispatch2_st<8, 2, 8, OP>(p, A, s);
+    case 2:
+    case 8:
+      return dispatch2_st<4, 4, 4, OP>(p, A, s);
+    case 4:
+    case 6:
+      return dispatch2_st<4, 2, 4, OP>(p, A, s);
+    case 7:
+      return dispatch2_st<2, 4, 2, OP>(p, A, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace pstm

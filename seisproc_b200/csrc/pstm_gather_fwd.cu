@@ -1,5 +1,5 @@
-// Instantiates the gather kernel for OP_FWD (one op per translation unit).
-#include "pstm_gather.cuh"
+// Instantiates the gather kernel for OP_FWD (warp-specialised pipeline; one op per translation unit).
+#include "pstm_gather2.cuh"
 
 namespace pstm {
 
@@ -7,7 +7,7 @@ pstm_status launch_forward(Plan* p, const float* vel, int64_t vst, int64_t vsc, 
                            cudaStream_t s, std::string* why) {
   KArgs A = make_args(p, vel, vst, vsc);
   A.out = image;
-  cudaError_t e = dispatch_shape<OP_FWD>(p, A, needs_lowclamp(p), s);
+  cudaError_t e = dispatch2_shape<OP_FWD>(p, A, s);
   return e == cudaSuccess ? PSTM_OK : cuda_fail(e, "forward kernel", why);
 }
 

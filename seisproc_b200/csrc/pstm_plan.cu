@@ -611,11 +611,13 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
     CUDA_TRY(cudaMalloc(&p->traces, bytes));
     p->bytes += (int64_t)bytes;
     CUDA_TRY(cudaMemsetAsync(p->traces, 0, bytes, s));
-    if (p->params.storage != PSTM_F32) CUDA_TRY(dalloc(p, &p->scales, n));
+    // f16 needs a per-trace scale for its range; bf16 has float32's exponent
+    // range and is stored unscaled
+    if (p->params.storage == PSTM_F16) CUDA_TRY(dalloc(p, &p->scales, n));
   }
   const int thr = 256;
-  if (p->params.storage != PSTM_F32) {
-    const float target = p->params.storage == PSTM_F16 ? 32768.0f : 1.0f;
+  if (p->params.storage == PSTM_F16) {
+    const float target = 32768.0f;
     maxabs_kernel<<<(unsigned)((n + thr - 1) / thr), thr, 0, s>>>(traces, n, n_s, trace_major,
                                                                   p->inv_perm, target, p->scales);
     LAUNCH_CHECK("maxabs_kernel");
