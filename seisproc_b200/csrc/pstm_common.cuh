@@ -104,26 +104,27 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+// A waiting thread is suspended by the hardware (up to the hint, in ns) until
+// the phase completes, so waiting warps do not spin on issue slots.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const uint32_t addr = smem_addr(bar);
+  const uint32_t hint_ns = 20000;
   uint64_t t0 = 0;
   for (uint32_t it = 0;; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(addr), "r"(parity)
+        : "r"(addr), "r"(parity), "r"(hint_ns)
         : "memory");
     if (done) return true;
-    if ((it & 63) == 0) {
-      const uint64_t now = global_ns();
-      if (it == 0)
-        t0 = now;
-      else if (now - t0 > PSTM_WAIT_NS)
-        return false;
-    }
+    const uint64_t now = global_ns();
+    if (it == 0)
+      t0 = now;
+    else if (now - t0 > PSTM_WAIT_NS)
+      return false;
   }
 }
 

@@ -12,21 +12,22 @@ from oracle import pstm_fp64 as O
 pytestmark = pytest.mark.gpu
 
 
-def _survey(seed=11, n_traces=1500, n_samples=160, aperture=400.0, angle=60.0, lateral=True):
+def _survey(seed=11, n_traces=1500, n_samples=160, aperture=400.0, angle=60.0, lateral=True,
+            **kw):
     from seisproc_b200 import synthetic
     return synthetic.survey_3d(n_traces=n_traces, seed=seed, n_samples=n_samples, extent=900.0,
                                max_offset=600.0, n_il=6, n_xl=5, spacing=25.0, n_diffractors=6,
-                               aperture=aperture, angle=angle, lateral_velocity=lateral)
+                               aperture=aperture, angle=angle, lateral_velocity=lateral, **kw)
 
 
-def _plan(s, **kw):
+def _plan(s, t0_ms=0.0, **kw):
     from seisproc_b200.kirchhoff import PSTMPlan
     dev = torch.device("cuda")
     c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
          for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
     return PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
                     origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
-                    xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                    xl_dy=s.xl_spacing, t0_ms=t0_ms, dt_ms=s.dt_ms, n_samples=s.n_samples,
                     in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
                     max_angle_deg=s.max_angle_deg, **kw)
 
@@ -80,10 +81,17 @@ def test_velocity_gradient_matches_fp64_oracle():
 
 def test_velocity_gradient_finite_differences():
     """Directional derivatives along 20 random V perturbations, central
-    differences with relative step 1e-3, against the gradient kernel."""
+    differences with relative step 1e-3, against the gradient kernel.
+
+    The forward operator is only piecewise smooth: linear interpolation has a
+    kink at every sample and the masks switch on and off.  The check therefore
+    uses band-limited noise-free data (8 Hz at 4 ms) and output times from
+    200 ms, where no mask changes under the perturbation; what remains is the
+    secant error of the interpolation kinks (~1e-3 .. 1e-2)."""
     from seisproc_b200.autograd import migrate
-    s = _survey(seed=14, aperture=5e4, angle=89.0)
-    plan = _plan(s)
+    s = _survey(seed=14, aperture=5e4, angle=89.0, n_samples=300, n_times=160, f_peak=8.0,
+                noise_rel=0.0)
+    plan = _plan(s, t0_ms=200.0)
     v0 = torch.from_numpy(s.vrms.astype(np.float64)).cuda()
     tr = s.traces.cuda()
     g = torch.from_numpy(np.random.RandomState(5).randn(*s.vrms.shape).astype(np.float32)).cuda()
@@ -99,7 +107,7 @@ def test_velocity_gradient_finite_differences():
         fd = (f(v0 + dv) - f(v0 - dv)) / 2.0
         an = float((grad * dv).sum())
         errs.append(abs(fd - an) / max(abs(fd), abs(an), 1e-30))
-    assert np.median(errs) <= 2e-2 and max(errs) <= 1e-1, errs
+    assert np.median(errs) <= 1e-2 and max(errs) <= 5e-2, errs
 
 
 def test_autograd_traces_gradient_is_demigration():
@@ -111,7 +119,9 @@ def test_autograd_traces_gradient_is_demigration():
     g = torch.randn(s.n_times, s.n_il, s.n_xl, device="cuda")
     (migrate(tr, v, plan) * g).sum().backward()
     ref = plan.demigrate(g, v)
-    assert torch.allclose(tr.grad, ref, rtol=1e-6, atol=0)
+    # same operator; the adjoint accumulates with float atomics, so the order
+    # of additions (and the last bits) may differ between two calls
+    assert rel_l2(tr.grad.cpu().numpy(), ref.cpu().numpy()) <= 1e-6
 
 
 def test_cgls_reduces_misfit():
