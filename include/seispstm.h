@@ -202,6 +202,36 @@ pstm_status pstm_normalize_mute(const float* image, const float* fold, float* ou
 /* Number of kernel launches issued by this library since load (for accounting). */
 int64_t pstm_launch_count(void);
 
+/* Size of the device scratch array used by pstm_migrate_noalloc. */
+#define PSTM_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* Forward migration + fold (as pstm_plan_create + pstm_migrate + pstm_check) that
+ * allocates no device memory.  It has no counterpart in the reference.
+ *
+ * It is for callers that must not allocate while they run.  Examples: a process
+ * whose caching allocator (PyTorch's, or an application's memory pool) already
+ * owns the device's free memory; a real-time path that cannot take the
+ * device-wide synchronisation cudaFree implies; code issuing work where
+ * allocation is not allowed.  The caller still passes the inputs (traces
+ * (n_samples, n_traces) float32 sample-major, coordinates, velocity) and the
+ * outputs (image, fold; fold may be NULL).
+ *
+ * Its scratch lives in one static device array of PSTM_NOALLOC_SCRATCH_BYTES,
+ * which every GPU that loads the library holds until the process exits.
+ * Problems that need more reject with PSTM_EINVAL.  The scratch holds the
+ * grid-local geometry (16 B/trace), the per-tile trace lists (sized for the
+ * worst case, 4 B per tile per trace) and the staged float32 trace rows;
+ * storage must be PSTM_F32.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress), so make it before any stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU race, and
+ * the array keeps the last call's contents (the error flag is cleared on every
+ * call).  The call synchronises `stream` before it returns, to report
+ * device-side errors. */
+pstm_status pstm_migrate_noalloc(const pstm_grid* grid, const pstm_params* params,
+                                 const pstm_geometry* geometry, const float* traces,
+                                 const float* velocity, int64_t v_stride_t, int64_t v_stride_c,
+                                 float* image, float* fold, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

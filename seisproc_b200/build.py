@@ -24,6 +24,7 @@ SOURCES = [
     "pstm_gather_fwd.cu",
     "pstm_gather_adj.cu",
     "pstm_gather_vgrad.cu",
+    "pstm_noalloc.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

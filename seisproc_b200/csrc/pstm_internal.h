@@ -67,5 +67,6 @@ pstm_status launch_velocity_check(Plan* p, const float* vel, int64_t vst, int64_
 bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out);
 size_t forward_smem_bytes(const Plan* p);
 void count_launch();
+void set_last_error(const std::string& msg);  // message returned by pstm_last_error
 
 }  // namespace pstm

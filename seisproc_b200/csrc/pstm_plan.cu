@@ -25,6 +25,8 @@ static pstm_status fail(pstm_status st, const std::string& msg) {
   return st;
 }
 
+void pstm::set_last_error(const std::string& msg) { g_last_error = msg; }
+
 #define CUDA_TRY(expr)                                                               \
   do {                                                                               \
     cudaError_t _e = (expr);                                                         \
