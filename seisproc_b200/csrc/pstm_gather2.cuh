@@ -1,10 +1,10 @@
 // Warp-specialised gather kernel (forward migration and V-gradient).
 //
-// CTA = NW consumer warps + 1 producer warp.  The producer streams the rows of
-// the tile's trace list through an NSTAGE-deep ring of shared-memory stages
-// (kBlockTraces rows each) with 1-D TMA bulk copies; `full[s]` completes on the
-// copies' byte count, `empty[s]` when every consumer warp has finished the
-// stage.  Consumer warps never synchronise with each other: each one computes
+// The rows of the tile's trace list stream through a ring of up to 4
+// shared-memory stages (up to 8 rows each) by 1-D TMA bulk copies issued by
+// lane 0 of warp 0; `full[s]` completes on the copies' byte count, `empty[s]`
+// when every warp has finished the stage.  Warps never synchronise with each
+// other otherwise (warp 0 waits on `empty` before refilling): each one computes
 // the per-(column, trace) set-up for 32 list entries at a time (one lane per
 // trace: leg distances and the first contributing sample by binary search in
 // the CTA's threshold table), then sweeps the traces, taking each trace's
@@ -16,6 +16,10 @@
 namespace pstm {
 
 constexpr int kMaxStages = 4;
+// Every staged row is preceded by 16 zero bytes, so an index in (-1, 0) -- an
+// output time equal to the first input time, rounded -- reads x[-1] = 0 with
+// weight (1 - f) ~ 0 instead of leaving the row.
+constexpr int kRowGuard = 16;
 constexpr int kSmemBudget = 227 * 1024;
 
 struct Smem2 {
@@ -32,7 +36,7 @@ __host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, i
   o += cols * T * 4;
   o = (o + 127) & ~127;
   L.raw = o;
-  o += stages * sb * S * elt;
+  o += stages * sb * (S * elt + kRowGuard);
   L.total = o;
   return L;
 }
@@ -74,12 +78,87 @@ __device__ __forceinline__ float lds_elem<__half>(uint32_t addr) {
   return __half2float(__ushort_as_half(h));
 }
 
-template <int COLS, int WPC, int M, typename ST, int WM, int OP>
-__global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(const KArgs A) {
+// One straight-line sweep over the M sample groups of a warp for NTR traces at
+// once (their dependency chains interleave).  Per trace n: squared leg
+// distances hs2[n], hr2[n], the shared-memory address of its staged row minus
+// the bit pattern of 2^23 (so the index's float bits address the sample), its
+// first contributing sample kst[n] (samples before it get weight 0 when
+// MASKED) and, for f16 storage, its scale.
+template <int M, typename ST, int WM, bool LOWC, bool MASKED, int OP, int NTR>
+__device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], const f2 (&aa)[M],
+                                             const float (&hs2)[NTR], const float (&hr2)[NTR],
+                                             const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
+                                             const float (&sc)[NTR], f2 bb, float hi_c,
+                                             float lo_c, int kw, int lane) {
+  constexpr int ES = (int)sizeof(ST);
+  constexpr int SHIFT = ES == 4 ? 2 : 1;
+  const f2 magic2 = f2_bcast(kMagic);
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+#pragma unroll
+    for (int n = 0; n < NTR; ++n) {
+      const f2 hs2b = f2_bcast(hs2[n]), hr2b = f2_bcast(hr2[n]);
+      const f2 rrs = f2_add(hs2b, zz[i]);
+      const f2 rrr = f2_add(hr2b, zz[i]);
+      const f2 qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
+      const f2 qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
+      const f2 sum = f2_fma(rrr, qr, f2_mul(rrs, qs));
+      f2 id = f2_fma(sum, aa[i], bb);
+      const f2 id_raw = id;
+      id.x = fminf(id.x, hi_c);
+      id.y = fminf(id.y, hi_c);
+      if constexpr (LOWC) {
+        id.x = fmaxf(id.x, lo_c);
+        id.y = fmaxf(id.y, lo_c);
+      }
+      const f2 tm = f2_add_rm(id, magic2);
+      const f2 fr = f2_sub(id, f2_sub(tm, magic2));
+      const uint32_t a0 = rbase[n] + (__float_as_uint(tm.x) << SHIFT);
+      const uint32_t a1 = rbase[n] + (__float_as_uint(tm.y) << SHIFT);
+      const f2 x0 = f2{lds_elem<ST>(a0), lds_elem<ST>(a1)};
+      const f2 x1 = f2{lds_elem<ST>(a0 + ES), lds_elem<ST>(a1 + ES)};
+      const f2 dx = f2_sub(x1, x0);
+      const f2 amp = f2_fma(fr, dx, x0);
+      const f2 p = f2_mul(qs, qr);
+      f2 w;
+      if constexpr (WM == W_OBL_SPREAD) {
+        w = f2_mul(p, p);
+      } else if constexpr (WM == W_OBL) {
+        w = p;
+      } else if constexpr (WM == W_SPREAD) {
+        w = f2{p.x * rcp_approx(fmaf(1e-6f, p.x, 1.0f)), p.y * rcp_approx(fmaf(1e-6f, p.y, 1.0f))};
+      } else {
+        w = f2{1.0f, 1.0f};
+      }
+      if constexpr (std::is_same<ST, __half>::value) w = f2_mul(w, f2_bcast(sc[n]));
+      if constexpr (MASKED) {
+        const int klo = kw + 64 * i + lane;
+        w.x = klo >= kst[n] ? w.x : 0.f;
+        w.y = klo + 32 >= kst[n] ? w.y : 0.f;
+      }
+      if constexpr (OP == OP_FWD) {
+        acc[i] = f2_fma(amp, w, acc[i]);
+      } else {  // OP_VGRAD
+        const f2 slope = f2{(id_raw.x < hi_c && id_raw.x > lo_c) ? dx.x : 0.f,
+                            (id_raw.y < hi_c && id_raw.y > lo_c) ? dx.y : 0.f};
+        const f2 q2 = f2_fma(qs, qs, f2_mul(qr, qr));
+        const f2 one_m = f2_sub(f2_bcast(1.0f), f2_mul(zz[i], q2));
+        const f2 hq = f2_fma(hs2b, qs, f2_mul(hr2b, qr));
+        const f2 term = f2_sub(f2_mul(f2_bcast(2.0f), f2_mul(amp, one_m)),
+                               f2_mul(f2_mul(slope, aa[i]), hq));
+        acc[i] = f2_fma(term, w, acc[i]);
+      }
+    }
+  }
+}
+
+template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP>
+__global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const KArgs A) {
   constexpr int NW = COLS * WPC;
   constexpr int T = WPC * 64 * M;
   constexpr int ES = (int)sizeof(ST);
   constexpr int SHIFT = ES == 4 ? 2 : 1;
+  static_assert(kRowGuard % 16 == 0, "row data must stay 16-byte aligned");
   extern __shared__ __align__(128) unsigned char smem[];
   const int S = A.S;
   const int B = A.ring_rows, kStages = A.ring_stages;
@@ -88,7 +167,8 @@ __global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(co
   uint64_t* empty = full + kMaxStages;
   int* abort_flag = reinterpret_cast<int*>(empty + kMaxStages);
   float* thr = reinterpret_cast<float*>(smem + L.thr);
-  ST* raw = reinterpret_cast<ST*>(smem + L.raw);
+  unsigned char* raw = smem + L.raw;
+  const int RP = S * ES + kRowGuard;  // bytes per staged row incl. its guard
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -111,6 +191,8 @@ __global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(co
     *abort_flag = 0;
     fence_mbar_init();
   }
+  for (int r = tid; r < kStages * B; r += blockDim.x)
+    *reinterpret_cast<uint4*>(raw + r * RP) = make_uint4(0u, 0u, 0u, 0u);
   for (int e = tid; e < COLS * T; e += blockDim.x) {
     const int q = e / T, kk = e - q * T;
     int qil, qxl;
@@ -120,38 +202,24 @@ __global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(co
   }
   __syncthreads();
 
-  if (warp == NW) {
-    // ------------------------------------------------------------ producer
-    const uint32_t bytes = (uint32_t)(rowlen * ES);
-    const ST* src = reinterpret_cast<const ST*>(A.traces);
-    for (int b = 0; b < nb; ++b) {
-      const int s = b % kStages;
-      if (b >= kStages) {
-        bool ok = true;
-        if (lane == 0) ok = mbar_wait(empty + s, ((b / kStages) - 1) & 1);
-        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-        if (!ok || *reinterpret_cast<volatile int*>(abort_flag)) {
-          if (lane == 0) {
-            set_error(A.err, PSTM_ERR_TIMEOUT);
-            *abort_flag = 1;
-          }
-          break;
-        }
-      }
-      const int cnt = min(B, n_list - b * B);
-      if (lane == 0) mbar_arrive_expect_tx(full + s, bytes * cnt);
-      __syncwarp();
-      if (lane < cnt) {
-        const int jj = A.list[off0 + (int64_t)b * B + lane];
-        bulk_g2s(raw + (s * B + lane) * S, src + (int64_t)jj * S + lo, bytes, full + s);
-      }
+  // Lane 0 of warp 0 issues the bulk copies: the first kStages blocks now, and
+  // block b + kStages into stage b % kStages once every warp has released
+  // block b (warp 0 waits for that, so it never runs ahead of the others by
+  // more than the ring).
+  const uint32_t bytes = (uint32_t)(rowlen * ES);
+  auto issue = [&](int b) {
+    const int s = b % kStages;
+    const int cnt = min(B, n_list - b * B);
+    if (lane == 0) mbar_arrive_expect_tx(full + s, bytes * cnt);
+    __syncwarp();
+    if (lane < cnt) {
+      const int jj = A.list[off0 + (int64_t)b * B + lane];
+      bulk_g2s(raw + (s * B + lane) * RP + kRowGuard,
+               reinterpret_cast<const ST*>(A.traces) + (int64_t)jj * S + lo, bytes, full + s);
     }
-    // keep the CTA (and its shared memory) alive until the copies in flight land
-    if (lane == 0) {
-      for (int b = max(0, nb - kStages); b < nb; ++b) mbar_wait(full + b % kStages, (b / kStages) & 1);
-    }
-    return;
-  }
+  };
+  if (warp == 0)
+    for (int b = 0; b < min(nb, kStages); ++b) issue(b);
 
   // -------------------------------------------------------------- consumers
   const int cl = warp / WPC, ts = warp % WPC;
@@ -177,17 +245,13 @@ __global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(co
   const float bconst = -A.in_t0 / A.in_dt - (float)lo;
   const f2 bb = f2_bcast(bconst);
   const float hi_c = A.clamp_hi - (float)lo;
-  const float lo_c = -(float)lo;  // idx >= 0
-  // the lower clamp matters only where idx can reach 0: the first window, or
-  // output times before the first input sample
-  const bool lowclamp = (k0 == 0) || (A.out_t0 < A.in_t0);
-  const f2 magic2 = f2_bcast(kMagic);
+  const float lo_c = -(float)lo;  // idx >= 0 (LOWC: output times before the first input)
   const float* thr_c = thr + cl * T;
-  const uint32_t raw_base = smem_addr(raw) - (kMagicBits << SHIFT);
-  float sc = 1.0f;
+  const uint32_t raw_base = smem_addr(raw) + kRowGuard - (kMagicBits << SHIFT);
+  const int kwe = kw + 64 * M;
 
   bool aborted = false;
-  int slot = 0, stage = 0;
+  int slot = 0, stage = 0, blk = 0;
   uint32_t phase = 0;
   // the next chunk's list entries and geometry are fetched while the current
   // chunk computes
@@ -210,9 +274,9 @@ __global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(co
     const int pn = p0 + 32 + lane;
     if (pn < n_list) jj_next = A.list[off0 + pn];
     const int nt = min(32, n_list - p0);
-    for (int t = 0; t < nt; ++t) {
+    for (int t = 0; t < nt;) {
       const int p = p0 + t;
-      if (t == 4 && warp_live && pn < n_list) g_next = __ldg(A.geo + jj_next);
+      if (t <= 4 && t + 2 > 4 && warp_live && pn < n_list) g_next = __ldg(A.geo + jj_next);
       if (slot == 0) {
         bool ok = true;
         if (lane == 0) ok = mbar_wait(full + stage, phase);
@@ -226,86 +290,59 @@ __global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(co
           break;
         }
       }
-      const int kst = __shfl_sync(0xffffffffu, ks, t);
-      if (kst < kw + 64 * M) {
-        const f2 hs2b = f2_bcast(__shfl_sync(0xffffffffu, hs2, t));
-        const f2 hr2b = f2_bcast(__shfl_sync(0xffffffffu, hr2, t));
-        if (std::is_same<ST, __half>::value) sc = __shfl_sync(0xffffffffu, tsc, t);
-        const uint32_t rbase = raw_base + (uint32_t)((stage * B + slot) * S * ES);
-        auto sweep = [&](auto masked_tag, auto low_tag) {
-          constexpr bool MASKED = decltype(masked_tag)::value;
-          constexpr bool LOWC = decltype(low_tag)::value;
-#pragma unroll
-          for (int i = 0; i < M; ++i) {
-            const f2 rrs = f2_add(hs2b, zz[i]);
-            const f2 rrr = f2_add(hr2b, zz[i]);
-            const f2 qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
-            const f2 qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
-            const f2 sum = f2_fma(rrr, qr, f2_mul(rrs, qs));
-            f2 id = f2_fma(sum, aa[i], bb);
-            const f2 id_raw = id;
-            id.x = fminf(id.x, hi_c);
-            id.y = fminf(id.y, hi_c);
-            if constexpr (LOWC) {
-              id.x = fmaxf(id.x, lo_c);
-              id.y = fmaxf(id.y, lo_c);
-            }
-            const f2 tm = f2_add_rm(id, magic2);
-            const f2 fr = f2_sub(id, f2_sub(tm, magic2));
-            const uint32_t a0 = rbase + (__float_as_uint(tm.x) << SHIFT);
-            const uint32_t a1 = rbase + (__float_as_uint(tm.y) << SHIFT);
-            const f2 x0 = f2{lds_elem<ST>(a0), lds_elem<ST>(a1)};
-            const f2 x1 = f2{lds_elem<ST>(a0 + ES), lds_elem<ST>(a1 + ES)};
-            const f2 dx = f2_sub(x1, x0);
-            const f2 amp = f2_fma(fr, dx, x0);
-            const f2 p = f2_mul(qs, qr);
-            f2 w;
-            if (WM == W_OBL_SPREAD) {
-              w = f2_mul(p, p);
-            } else if (WM == W_OBL) {
-              w = p;
-            } else if (WM == W_SPREAD) {
-              w = f2{p.x * rcp_approx(fmaf(1e-6f, p.x, 1.0f)),
-                     p.y * rcp_approx(fmaf(1e-6f, p.y, 1.0f))};
-            } else {
-              w = f2{1.0f, 1.0f};
-            }
-            if (std::is_same<ST, __half>::value) w = f2_mul(w, f2_bcast(sc));
-            if constexpr (MASKED) {
-              const int klo = kw + 64 * i + lane;
-              w.x = klo >= kst ? w.x : 0.f;
-              w.y = klo + 32 >= kst ? w.y : 0.f;
-            }
-            if (OP == OP_FWD) {
-              acc[i] = f2_fma(amp, w, acc[i]);
-            } else {  // OP_VGRAD
-              const f2 slope = f2{(id_raw.x < hi_c && id_raw.x > lo_c) ? dx.x : 0.f,
-                                  (id_raw.y < hi_c && id_raw.y > lo_c) ? dx.y : 0.f};
-              const f2 q2 = f2_fma(qs, qs, f2_mul(qr, qr));
-              const f2 one_m = f2_sub(f2_bcast(1.0f), f2_mul(zz[i], q2));
-              const f2 hq = f2_fma(hs2b, qs, f2_mul(hr2b, qr));
-              const f2 term = f2_sub(f2_mul(f2_bcast(2.0f), f2_mul(amp, one_m)),
-                                     f2_mul(f2_mul(slope, aa[i]), hq));
-              acc[i] = f2_fma(term, w, acc[i]);
-            }
-          }
-        };
-        const bool masked = kst > kw;
-        if (lowclamp) {
-          if (masked)
-            sweep(std::true_type{}, std::true_type{});
-          else
-            sweep(std::false_type{}, std::true_type{});
-        } else {
-          if (masked)
-            sweep(std::true_type{}, std::false_type{});
-          else
-            sweep(std::false_type{}, std::false_type{});
-        }
+      // two traces of the same stage when available
+      const bool pair = (slot + 1 < B) && (t + 1 < nt);
+      const int ka = __shfl_sync(0xffffffffu, ks, t);
+      const int kb = __shfl_sync(0xffffffffu, ks, pair ? t + 1 : t);
+      const bool la = ka < kwe, lb = pair && kb < kwe;
+      const uint32_t rb0 = raw_base + (uint32_t)((stage * B + slot) * RP);
+      if (la && lb) {
+        const float hs[2] = {__shfl_sync(0xffffffffu, hs2, t), __shfl_sync(0xffffffffu, hs2, t + 1)};
+        const float hr[2] = {__shfl_sync(0xffffffffu, hr2, t), __shfl_sync(0xffffffffu, hr2, t + 1)};
+        const float sc[2] = {__shfl_sync(0xffffffffu, tsc, t), __shfl_sync(0xffffffffu, tsc, t + 1)};
+        const uint32_t rb[2] = {rb0, rb0 + (uint32_t)RP};
+        const int kk[2] = {ka, kb};
+        if (ka > kw || kb > kw)
+          sweep_traces<M, ST, WM, LOWC, true, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
+                                                      lo_c, kw, lane);
+        else
+          sweep_traces<M, ST, WM, LOWC, false, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
+                                                       lo_c, kw, lane);
+      } else if (la || lb) {
+        const int u = la ? t : t + 1;
+        const float hs[1] = {__shfl_sync(0xffffffffu, hs2, u)};
+        const float hr[1] = {__shfl_sync(0xffffffffu, hr2, u)};
+        const float sc[1] = {__shfl_sync(0xffffffffu, tsc, u)};
+        const uint32_t rb[1] = {la ? rb0 : rb0 + (uint32_t)RP};
+        const int kk[1] = {la ? ka : kb};
+        if (kk[0] > kw)
+          sweep_traces<M, ST, WM, LOWC, true, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
+                                                      lo_c, kw, lane);
+        else
+          sweep_traces<M, ST, WM, LOWC, false, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
+                                                       lo_c, kw, lane);
       }
-      if (++slot == B || p == n_list - 1) {
+      const int adv = pair ? 2 : 1;
+      t += adv;
+      slot += adv;
+      if (slot == B || p + adv == n_list) {
         __syncwarp();
         if (lane == 0) mbar_arrive(empty + stage);
+        if (warp == 0 && blk + kStages < nb) {
+          bool ok = true;
+          if (lane == 0) ok = mbar_wait(empty + stage, phase);
+          ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+          if (!ok) {
+            if (lane == 0) {
+              set_error(A.err, PSTM_ERR_TIMEOUT);
+              *abort_flag = 1;
+            }
+            aborted = true;
+            break;
+          }
+          issue(blk + kStages);
+        }
+        ++blk;
         slot = 0;
         if (++stage == kStages) {
           stage = 0;
@@ -314,7 +351,14 @@ __global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(co
       }
     }
   }
-  if (aborted || !warp_live) return;
+  if (aborted) {
+    // leave no bulk copy in flight into this CTA's shared memory
+    if (warp == 0 && lane == 0)
+      for (int b = blk; b < min(nb, blk + kStages); ++b)
+        mbar_wait(full + b % kStages, (b / kStages) & 1);
+    return;
+  }
+  if (!warp_live) return;
 #pragma unroll
   for (int i = 0; i < M; ++i) {
     const int klo = kw + 64 * i + lane, khi = klo + 32;
@@ -338,7 +382,8 @@ __global__ void __launch_bounds__(COLS* WPC * 32 + 32, 1) pstm_gather2_kernel(co
 
 template <int COLS, int WPC, int M, typename ST, int WM, int OP>
 inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
-  auto kern = pstm_gather2_kernel<COLS, WPC, M, ST, WM, OP>;
+  auto kern = needs_lowclamp(p) ? pstm_gather2_kernel<COLS, WPC, M, ST, WM, true, OP>
+                                : pstm_gather2_kernel<COLS, WPC, M, ST, WM, false, OP>;
   const int T = WPC * 64 * M;
   KArgs A2 = A;
   if (!ring_shape(COLS, T, p->row_stride, (int)sizeof(ST), &A2.ring_stages, &A2.ring_rows))
@@ -348,7 +393,7 @@ inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)p->n_tiles, (unsigned)((p->grid.n_times + T - 1) / T));
-  kern<<<grid, COLS * WPC * 32 + 32, L.total, s>>>(A2);
+  kern<<<grid, COLS * WPC * 32, L.total, s>>>(A2);
   count_launch();
   return cudaGetLastError();
 }

@@ -100,14 +100,16 @@ def test_velocity_gradient_finite_differences():
     (img * g).sum().backward()
     grad = vv.grad.double()
     rs = np.random.RandomState(6)
-    errs = []
+    fds, ans = [], []
     for _ in range(20):
         dv = torch.from_numpy(rs.randn(*s.vrms.shape)).cuda() * v0 * 1e-3
         f = lambda vx: float((migrate(tr, vx.float(), plan).double() * g.double()).sum())
-        fd = (f(v0 + dv) - f(v0 - dv)) / 2.0
-        an = float((grad * dv).sum())
-        errs.append(abs(fd - an) / max(abs(fd), abs(an), 1e-30))
-    assert np.median(errs) <= 1e-2 and max(errs) <= 5e-2, errs
+        fds.append((f(v0 + dv) - f(v0 - dv)) / 2.0)
+        ans.append(float((grad * dv).sum()))
+    fds, ans = np.array(fds), np.array(ans)
+    # aggregate over the 20 directions: single directions whose derivative is
+    # small are dominated by float32 rounding of the two forward runs
+    assert np.linalg.norm(fds - ans) / np.linalg.norm(fds) <= 2e-2, (fds, ans)
 
 
 def test_autograd_traces_gradient_is_demigration():
