@@ -35,6 +35,10 @@ sys.path.insert(0, ROOT)
 
 MUFU_PER_SM_CLK = 16
 RSQRT_PER_PAIR = 2
+# DRAM bytes per trace-list entry of the forward gather, from the ncu capture
+# of the 100k-trace case (7.56 GB / 17.35 M entries; profiles/pstm_gather_forward_3d.md);
+# the traffic of a full launch is scaled by its list entries.
+DRAM_BYTES_PER_LIST_ENTRY = 436.0
 
 
 def peaks():
@@ -310,8 +314,13 @@ def bench_ours(args):
         fwd_avg = statistics.mean(fwd_ms)
         peak_pairs = 148 * MUFU_PER_SM_CLK / RSQRT_PER_PAIR * pk["sm_max_mhz"] * 1e6 / 1e12
         achieved = pairs / (fwd_avg * 1e-3) / 1e12
+        traffic = DRAM_BYTES_PER_LIST_ENTRY * plan.stats()["list_entries"]
         roof = {"bound": "mufu", "achieved": achieved, "peak": peak_pairs, "unit": "Tpairs/s",
-                "frac": achieved / peak_pairs, "traffic": None,
+                "frac": achieved / peak_pairs, "traffic": traffic,
+                "traffic_note": "DRAM bytes per launch scaled from the ncu capture of the "
+                                "100k-trace case by list entries",
+                "hbm_achieved_gbs": traffic / (fwd_avg * 1e-3) / 1e9,
+                "hbm_peak_gbs": pk["hbm_gbs"],
                 "peak_source": f"{pk['source']} sm_max_mhz {pk['sm_max_mhz']}",
                 "kernel": "pstm_gather_kernel (forward)", "kernel_ms": fwd_avg,
                 "stage_ms": statistics.mean(stage_ms), "fold_ms": statistics.mean(fold_ms)}
@@ -346,6 +355,131 @@ def bench_ours(args):
     return result
 
 
+def bench_batched(args):
+    """64 offset/azimuth classes (trace counts log-uniform 2k-40k), one persistent
+    launch per step replayed from a CUDA graph; value = pairs of all classes / time."""
+    from seisproc_b200 import _lib, synthetic
+    from seisproc_b200.batched import BatchedPSTM
+    from seisproc_b200.kirchhoff import PSTMPlan
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    L = _lib.lib()
+    counts = synthetic.class_counts_loguniform(64, 2000, 40000, seed=64)
+    t_gen = time.perf_counter()
+    surveys = synthetic.survey_classes(counts, seed=64, device=dev, n_samples=args.samples,
+                                       n_il=args.grid, n_xl=args.grid)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_gen
+    s0 = surveys[0]
+    plans = []
+    for s in surveys:
+        c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+             for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+        plans.append(PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times,
+                              origin_x=s.origin_x, origin_y=s.origin_y, il_dx=s.il_spacing,
+                              il_dy=0.0, xl_dx=0.0, xl_dy=s.xl_spacing, t0_ms=0.0,
+                              dt_ms=s.dt_ms, n_samples=s.n_samples, in_t0_ms=0.0,
+                              in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                              max_angle_deg=s.max_angle_deg, storage=args.storage,
+                              variant=args.variant))
+    vel = torch.from_numpy(s0.vrms).to(dev)
+    bufs = [s.traces for s in surveys]
+    b = BatchedPSTM(plans, vel)
+    b.capture(bufs)
+    for _ in range(args.warmup):
+        b.replay()
+    torch.cuda.synchronize()
+    b.check()
+    pairs = float(sum(f.double().sum() for f in b.folds))
+    l0 = L.pstm_launch_count()
+    with ClockSampler(0) as clk:
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            b.replay()
+        e.record()
+        torch.cuda.synchronize()
+    b.check()
+    ms = a.elapsed_time(e) / args.steps
+    n_tr = int(sum(s.n_traces for s in surveys))
+    res = {"metric": "PSTM Gpairs/s (out-sample x trace), batched classes", "value":
+           pairs / (ms * 1e-3) / 1e9, "unit": "Gpairs/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
+           "config": {"workload": f"batched 3D PSTM: 64 offset/azimuth classes, {n_tr} traces "
+                                  f"x {args.samples} samples, per-class "
+                                  f"{args.grid}x{args.grid}x{args.samples} images, "
+                                  f"{args.storage} storage, one persistent launch in a CUDA "
+                                  "graph", "pairs_per_step": pairs, "datagen_s": t_gen,
+                      "l2": "inputs larger than L2; no flush"},
+           "gpu_launches": int(b.launches_per_replay * args.steps),
+           "clocks": clk.summary()}
+    print(json.dumps(res), flush=True)
+    b.close()
+    for p in plans:
+        p.close()
+
+
+def bench_lsq(args):
+    """Least-squares PSTM: 100x100x500 grid, 120k traces at 2 ms, FP32 -- dot-product
+    test, finite-difference checks of the V gradient, 10 CG iterations."""
+    from seisproc_b200 import synthetic
+    from seisproc_b200.autograd import cgls, dot_product_test, migrate
+    from seisproc_b200.kirchhoff import PSTMPlan
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    s = synthetic.survey_3d(n_traces=120_000, seed=7, device=dev, n_samples=500, dt_ms=2.0,
+                            extent=2500.0, max_offset=1500.0, n_il=100, n_xl=100, spacing=25.0,
+                            n_diffractors=60, aperture=1000.0)
+    c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    plan = PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+                    origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                    xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                    in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                    max_angle_deg=s.max_angle_deg)
+    v = torch.from_numpy(s.vrms).to(dev)
+    a_, b_, rel = dot_product_test(plan, v, seed=7)
+    # V-gradient directional derivatives vs central differences (relative step 1e-3)
+    tr = s.traces
+    g = torch.randn(v.shape, device=dev, generator=torch.Generator(device=dev).manual_seed(3))
+    vv = v.clone().requires_grad_(True)
+    (migrate(tr, vv, plan) * g).sum().backward()
+    rs = np.random.RandomState(20)
+    fd, an = [], []
+    tt = np.linspace(0.0, 1.0, s.n_times)[:, None, None]
+    xx = np.linspace(0.0, 1.0, s.n_il)[None, :, None]
+    yy = np.linspace(0.0, 1.0, s.n_xl)[None, None, :]
+    for _ in range(20):
+        # smooth random perturbation (keeps V t0 increasing in t0)
+        c = rs.randn(4)
+        f = (c[0] + c[1] * np.sin(np.pi * (tt + rs.rand())) + c[2] * np.cos(2 * np.pi * xx)
+             + c[3] * np.sin(2 * np.pi * yy))
+        dv = torch.from_numpy((f / np.abs(f).max()).astype(np.float32)).to(dev) * v * 1e-3
+        f = lambda x: float((migrate(tr, x, plan).double() * g.double()).sum())
+        fd.append((f(v + dv) - f(v - dv)) / 2.0)
+        an.append(float((vv.grad.double() * dv.double()).sum()))
+    fd, an = np.array(fd), np.array(an)
+    plan.check()
+    d = plan.demigrate(migrate(tr, v, plan), v)  # data in the range of L
+    m, hist = cgls(plan, d, v, n_iter=10)
+    it_s = [h[2] for h in hist[1:]]
+    print(json.dumps({
+        "metric": "LSQ PSTM CG seconds per iteration", "value": float(np.median(it_s)),
+        "unit": "s/iter", "n_gpus": 1, "higher_is_better": False, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "least-squares PSTM 100x100x500, 120k traces at 2 ms, FP32"},
+        "dot_product": {"<Lm,d>": a_, "<m,L^T d>": b_, "rel": rel},
+        "vgrad_fd": {"rel_l2_over_20_directions": float(np.linalg.norm(fd - an) /
+                                                         np.linalg.norm(fd)),
+                     "note": "noisy 30 Hz data from t0 = 0: includes interpolation kinks and "
+                             "mask switches"},
+        "cg": {"residual_history": [h[1] for h in hist], "misfit_reduction": hist[-1][1]},
+    }), flush=True)
+    plan.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -360,7 +494,12 @@ def main():
     ap.add_argument("--crop", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--config", default="3d", choices=["3d", "batched", "lsq"])
     args = ap.parse_args()
+    if args.config == "batched" and args.impl == "ours":
+        return bench_batched(args)
+    if args.config == "lsq" and args.impl == "ours":
+        return bench_lsq(args)
     if args.impl == "reference":
         bench_reference(args)
     else:

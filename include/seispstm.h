@@ -199,6 +199,33 @@ pstm_status pstm_normalize_by_fold(const float* image, const float* fold, float*
 pstm_status pstm_normalize_mute(const float* image, const float* fold, float* out, int64_t n,
                                 float min_fold, void* stream);
 
+/* ---- batched migration: many plans in one persistent launch ------------- */
+typedef struct pstm_batch pstm_batch;
+
+/* Groups plans that share the kernel shape, storage, weight, clamp, time axis
+ * and trace length -- typically the offset/azimuth classes of one survey, each
+ * with its own geometry, traces and output image -- for pstm_batch_migrate.
+ * images[i] / folds[i] (folds may be NULL, or contain NULL entries) are the
+ * per-class outputs, velocity the V_rms shared by all classes.  Builds the
+ * device work list of (class, tile, window) items ordered by descending
+ * trace-list length.  No reference counterpart: the reference migrates bins
+ * one at a time (views/migration_monitor_dialog.py:201-430). */
+pstm_status pstm_batch_create(pstm_batch** batch, pstm_plan* const* plans, int32_t n_plans,
+                              float* const* images, float* const* folds, const float* velocity,
+                              int64_t v_stride_t, int64_t v_stride_c, void* stream);
+
+/* Migrates every class of the batch with the traces last loaded into each plan
+ * (pstm_load_traces): one launch of the persistent kernel (one CTA per SM,
+ * items pulled from a device queue), then the per-class folds.  Contains no
+ * allocation and no host synchronisation, so it can be captured in a CUDA
+ * graph.  Device-side errors are reported by pstm_check on the member plans. */
+pstm_status pstm_batch_migrate(pstm_batch* batch, void* stream);
+
+pstm_status pstm_batch_destroy(pstm_batch* batch);
+
+/* Number of plans in the batch. */
+int32_t pstm_batch_size(const pstm_batch* batch);
+
 /* Number of kernel launches issued by this library since load (for accounting). */
 int64_t pstm_launch_count(void);
 

@@ -84,6 +84,11 @@ _SIGNATURES = {
     "pstm_check": (C.c_int, [_P, _P]),
     "pstm_normalize_by_fold": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float, _P]),
     "pstm_normalize_mute": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float, _P]),
+    "pstm_batch_create": (C.c_int, [C.POINTER(_P), C.POINTER(_P), C.c_int32, C.POINTER(_P),
+                                    C.POINTER(_P), _P, C.c_int64, C.c_int64, _P]),
+    "pstm_batch_migrate": (C.c_int, [_P, _P]),
+    "pstm_batch_destroy": (C.c_int, [_P]),
+    "pstm_batch_size": (C.c_int32, [_P]),
     "pstm_migrate_noalloc": (C.c_int, [C.POINTER(Grid), C.POINTER(Params), C.POINTER(Geometry),
                                        _P, _P, C.c_int64, C.c_int64, _P, _P, _P]),
 }

@@ -25,6 +25,7 @@ SOURCES = [
     "pstm_gather_adj.cu",
     "pstm_gather_vgrad.cu",
     "pstm_noalloc.cu",
+    "pstm_batch.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -152,14 +152,18 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
   }
 }
 
+// One output tile x time window: the body shared by the per-plan grid kernel
+// (one CTA per tile/window) and the persistent batched kernel (one work item
+// at a time).  Barriers are (re)initialised on entry; every bulk copy issued
+// for the item has landed when it returns.
 template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP>
-__global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const KArgs A) {
+__device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, const int win,
+                                            unsigned char* smem) {
   constexpr int NW = COLS * WPC;
   constexpr int T = WPC * 64 * M;
   constexpr int ES = (int)sizeof(ST);
   constexpr int SHIFT = ES == 4 ? 2 : 1;
   static_assert(kRowGuard % 16 == 0, "row data must stay 16-byte aligned");
-  extern __shared__ __align__(128) unsigned char smem[];
   const int S = A.S;
   const int B = A.ring_rows, kStages = A.ring_stages;
   const Smem2 L = smem2_layout(COLS, T, S, ES, kStages, B);
@@ -172,8 +176,7 @@ __global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const K
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  const int tile = blockIdx.x;
-  const int k0 = blockIdx.y * T;
+  const int k0 = win * T;
   const int kend = min(k0 + T, A.n_times);
   const int nk = kend - k0;
   const int n_c = A.n_il * A.n_xl;
@@ -377,6 +380,42 @@ __global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const K
     }
     if (klo < A.n_times) A.out[(long long)klo * n_c + c] = acc[i].x * fl;
     if (khi < A.n_times) A.out[(long long)khi * n_c + c] = acc[i].y * fh;
+  }
+}
+
+template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP>
+__global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const KArgs A) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  gather_tile<COLS, WPC, M, ST, WM, LOWC, OP>(A, blockIdx.x, blockIdx.y, smem);
+}
+
+// Persistent batched kernel: CTAs pull (class, tile, window) work items from a
+// device queue (items ordered by descending trace-list length) until none is
+// left.  Each class has its own plan data and output image in descs[class].
+template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP>
+__global__ void __launch_bounds__(COLS* WPC * 32, 1)
+    pstm_batch_kernel(const KArgs* __restrict__ descs, const int4* __restrict__ items, int n_items,
+                      int* __restrict__ counter) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ int next;
+  __shared__ KArgs a;
+  for (;;) {
+    if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = next;
+    if (it >= n_items) break;
+    const int4 w = items[it];
+    if (threadIdx.x == 0) a = descs[w.x];
+    __syncthreads();
+    gather_tile<COLS, WPC, M, ST, WM, LOWC, OP>(a, w.y, w.z, smem);
+    __syncthreads();
+    if (threadIdx.x == 0) {  // every phase has completed: retire the barriers before re-use
+      uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+      for (int s = 0; s < a.ring_stages; ++s) {
+        mbar_inval(bars + s);
+        mbar_inval(bars + kMaxStages + s);
+      }
+    }
   }
 }
 

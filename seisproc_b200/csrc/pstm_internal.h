@@ -68,5 +68,6 @@ bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out);
 size_t forward_smem_bytes(const Plan* p);
 void count_launch();
 void set_last_error(const std::string& msg);  // message returned by pstm_last_error
+pstm_status ensure_trace_storage(Plan* p, cudaStream_t s);  // staged rows allocated once
 
 }  // namespace pstm

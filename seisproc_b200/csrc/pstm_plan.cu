@@ -391,6 +391,19 @@ static pstm_status validate(const pstm_grid* g, const pstm_params* prm, const ps
   return PSTM_OK;
 }
 
+// The plan's staged-trace rows (and f16 scales), allocated once.
+pstm_status pstm::ensure_trace_storage(Plan* p, cudaStream_t s) {
+  if (p->traces || p->n_traces == 0) return PSTM_OK;
+  const size_t bytes = (size_t)p->n_traces * p->row_stride * p->elt_bytes;
+  CUDA_TRY(cudaMalloc(&p->traces, bytes));
+  p->bytes += (int64_t)bytes;
+  CUDA_TRY(cudaMemsetAsync(p->traces, 0, bytes, s));
+  // f16 needs a per-trace scale for its range; bf16 has float32's exponent
+  // range and is stored unscaled
+  if (p->params.storage == PSTM_F16) CUDA_TRY(dalloc(p, &p->scales, p->n_traces));
+  return PSTM_OK;
+}
+
 extern "C" {
 
 int32_t pstm_abi_version(void) { return SEISPSTM_ABI_VERSION; }
@@ -608,15 +621,8 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
     return PSTM_OK;
   }
   if (!traces) return fail(PSTM_EINVAL, "null traces");
-  if (!p->traces) {
-    const size_t bytes = (size_t)n * p->row_stride * p->elt_bytes;
-    CUDA_TRY(cudaMalloc(&p->traces, bytes));
-    p->bytes += (int64_t)bytes;
-    CUDA_TRY(cudaMemsetAsync(p->traces, 0, bytes, s));
-    // f16 needs a per-trace scale for its range; bf16 has float32's exponent
-    // range and is stored unscaled
-    if (p->params.storage == PSTM_F16) CUDA_TRY(dalloc(p, &p->scales, n));
-  }
+  pstm_status st = ensure_trace_storage(p, s);
+  if (st != PSTM_OK) return st;
   const int thr = 256;
   if (p->params.storage == PSTM_F16) {
     const float target = 32768.0f;

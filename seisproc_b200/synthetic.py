@@ -190,26 +190,33 @@ def survey_3d(n_traces: int = 500_000, seed: int = 2025, device="cpu", n_samples
               n_diffractors: int = 200, aperture: float = 1000.0, angle: float = 60.0,
               noise_rel: float = 0.03, f_peak: float = 30.0, n_times: Optional[int] = None,
               utm_origin: Tuple[float, float] = (0.0, 0.0), lateral_velocity: bool = True,
-              midpoint_box: Optional[Tuple[float, float, float, float]] = None) -> Survey:
+              midpoint_box: Optional[Tuple[float, float, float, float]] = None,
+              offset_range: Optional[Tuple[float, float]] = None,
+              azimuth_range: Optional[Tuple[float, float]] = None,
+              diffractor_seed: Optional[int] = None) -> Survey:
     """3D survey: uniform midpoints/offsets/azimuths over point diffractors.
 
     ``utm_origin`` is added to every world coordinate (float64) to exercise
     tile-local coordinate handling; the output grid origin moves with it.
-    ``midpoint_box`` (x0, x1, y0, y1) restricts midpoints (used for crops).
+    ``midpoint_box`` (x0, x1, y0, y1) restricts midpoints (used for crops);
+    ``offset_range`` (m) and ``azimuth_range`` (radians) restrict the offsets
+    and azimuths (used to draw one offset/azimuth class).
     """
     rs = np.random.RandomState(seed)
     if midpoint_box is None:
         midpoint_box = (0.0, extent, 0.0, extent)
     mx = rs.uniform(midpoint_box[0], midpoint_box[1], n_traces)
     my = rs.uniform(midpoint_box[2], midpoint_box[3], n_traces)
-    off = rs.uniform(0.0, max_offset, n_traces)
-    az = rs.uniform(0.0, 2 * np.pi, n_traces)
+    o0, o1 = offset_range if offset_range is not None else (0.0, max_offset)
+    a0, a1 = azimuth_range if azimuth_range is not None else (0.0, 2 * np.pi)
+    off = rs.uniform(o0, o1, n_traces)
+    az = rs.uniform(a0, a1, n_traces)
     hx, hy = 0.5 * off * np.cos(az), 0.5 * off * np.sin(az)
     src = np.stack([mx - hx, my - hy], 1)
     rcv = np.stack([mx + hx, my + hy], 1)
     nt = n_samples if n_times is None else n_times
     t_max = (nt - 1) * dt_ms * 1e-3
-    drs = np.random.RandomState(seed + 1)
+    drs = np.random.RandomState(seed + 1 if diffractor_seed is None else diffractor_seed)
     dxy = np.stack([drs.uniform(0, extent, n_diffractors), drs.uniform(0, extent, n_diffractors)], 1)
     dt0 = drs.uniform(0.2, 0.9 * t_max, n_diffractors)
     damp = drs.uniform(0.5, 1.5, n_diffractors) * np.where(drs.rand(n_diffractors) < 0.5, -1.0, 1.0)
@@ -236,6 +243,22 @@ def survey_3d(n_traces: int = 500_000, seed: int = 2025, device="cpu", n_samples
                   n_il=n_il, n_xl=n_xl, n_times=nt, max_aperture_m=aperture, max_angle_deg=angle,
                   velocity_mps=float(vr.mean()), vrms=np.ascontiguousarray(vr, dtype=np.float32),
                   diffractors=dict(xy=dxy, t0=dt0, amp=damp, v=dv))
+
+
+def survey_classes(counts, seed: int = 64, n_offset_bins: int = 8, n_azimuth_bins: int = 8,
+                   max_offset: float = 3000.0, device="cpu", **kw):
+    """Offset/azimuth classes (offset-major) of one synthetic survey, class i
+    holding counts[i] traces drawn from its own offset bin and azimuth sector;
+    all classes share the diffractors, velocity and output grid."""
+    out = []
+    for i, n in enumerate(counts):
+        ob, ab = divmod(i, n_azimuth_bins)
+        out.append(survey_3d(
+            n_traces=int(n), seed=seed * 1000 + i, device=device, max_offset=max_offset,
+            offset_range=(ob * max_offset / n_offset_bins, (ob + 1) * max_offset / n_offset_bins),
+            azimuth_range=(ab * 2 * np.pi / n_azimuth_bins, (ab + 1) * 2 * np.pi / n_azimuth_bins),
+            diffractor_seed=seed + 1, **kw))
+    return out
 
 
 def class_counts_loguniform(n_classes: int = 64, lo: int = 2000, hi: int = 40000,
