@@ -141,6 +141,10 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
       free_batch(b);
       return bfail(PSTM_EINVAL, "null plan or image in batch");
     }
+    if (p->params.antialias) {
+      free_batch(b);
+      return bfail(PSTM_ENOTSUP, "the batched launch is built for the plain operator");
+    }
     // the descriptors capture the staging buffers, so they must exist now
     const pstm_status st = ensure_trace_storage(p, s);
     if (st != PSTM_OK) {

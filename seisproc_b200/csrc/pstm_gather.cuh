@@ -33,6 +33,9 @@ struct KArgs {
   float* accum;
   int* err;
   int ring_stages, ring_rows;  // pipelined kernel: stages x rows per stage
+  // anti-alias: output spacing (m) per axis, max half-width (samples), row pad
+  float aa_dx, aa_dy, aa_lmax;
+  int aa_pad;
 };
 
 __device__ __forceinline__ float vel_at(const KArgs& A, int k, int c) {
@@ -458,6 +461,11 @@ inline KArgs make_args(const Plan* p, const float* vel, int64_t vst, int64_t vsc
   A.in_img = nullptr;
   A.accum = p->accum;
   A.err = p->err;
+  A.ring_stages = A.ring_rows = 0;
+  A.aa_dx = (float)p->params.aa_dx;
+  A.aa_dy = (float)p->params.aa_dy;
+  A.aa_lmax = (float)p->params.aa_max_halfwidth;
+  A.aa_pad = p->aa_pad;
   return A;
 }
 

@@ -156,7 +156,69 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
 // (one CTA per tile/window) and the persistent batched kernel (one work item
 // at a time).  Barriers are (re)initialised on entry; every bulk copy issued
 // for the item has landed when it returns.
-template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP>
+// Anti-aliased sweep (float32 rows of the trend-removed double integral I2):
+// per sample the triangle half-width L = clamp(a * max(|gx|, |gy|), 1, Lmax)
+// with gx = (x - s_x) dx q_s + (x - r_x) dx q_r (the operator dip along the
+// inline axis times the inline spacing; gy likewise), then
+//   amp = (I2(idx + L) - 2 I2(idx) + I2(idx - L)) / L^2
+// from three linearly interpolated taps on the staged row.
+template <int M, bool LOWC, bool MASKED, int NTR>
+__device__ __forceinline__ void sweep_aa(f2 (&acc)[M], const f2 (&zz)[M], const f2 (&aa)[M],
+                                         const float (&hs2)[NTR], const float (&hr2)[NTR],
+                                         const float (&gxs)[NTR], const float (&gxr)[NTR],
+                                         const float (&gys)[NTR], const float (&gyr)[NTR],
+                                         const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
+                                         f2 bb, float hi_c, float lo_c, float lmax, int kw,
+                                         int lane) {
+  const f2 magic2 = f2_bcast(kMagic);
+  auto tap = [&](f2 pos, uint32_t base) {
+    const f2 tm = f2_add_rm(pos, magic2);
+    const f2 fr = f2_sub(pos, f2_sub(tm, magic2));
+    const uint32_t a0 = base + (__float_as_uint(tm.x) << 2);
+    const uint32_t a1 = base + (__float_as_uint(tm.y) << 2);
+    const f2 x0 = f2{lds_elem<float>(a0), lds_elem<float>(a1)};
+    const f2 x1 = f2{lds_elem<float>(a0 + 4), lds_elem<float>(a1 + 4)};
+    return f2_fma(fr, f2_sub(x1, x0), x0);
+  };
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+#pragma unroll
+    for (int n = 0; n < NTR; ++n) {
+      const f2 rrs = f2_add(f2_bcast(hs2[n]), zz[i]);
+      const f2 rrr = f2_add(f2_bcast(hr2[n]), zz[i]);
+      const f2 qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
+      const f2 qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
+      const f2 sum = f2_fma(rrr, qr, f2_mul(rrs, qs));
+      f2 id = f2_fma(sum, aa[i], bb);
+      id.x = fminf(id.x, hi_c);
+      id.y = fminf(id.y, hi_c);
+      if constexpr (LOWC) {
+        id.x = fmaxf(id.x, lo_c);
+        id.y = fmaxf(id.y, lo_c);
+      }
+      const f2 gx = f2_fma(f2_bcast(gxs[n]), qs, f2_mul(f2_bcast(gxr[n]), qr));
+      const f2 gy = f2_fma(f2_bcast(gys[n]), qs, f2_mul(f2_bcast(gyr[n]), qr));
+      f2 L = f2_mul(f2{fmaxf(fabsf(gx.x), fabsf(gy.x)), fmaxf(fabsf(gx.y), fabsf(gy.y))}, aa[i]);
+      L.x = fminf(fmaxf(L.x, 1.0f), lmax);
+      L.y = fminf(fmaxf(L.y, 1.0f), lmax);
+      const f2 il = f2{rcp_approx(L.x), rcp_approx(L.y)};
+      const f2 y0 = tap(f2_sub(id, L), rbase[n]);
+      const f2 y1 = tap(id, rbase[n]);
+      const f2 y2 = tap(f2_add(id, L), rbase[n]);
+      const f2 amp = f2_mul(f2_fma(f2_bcast(-2.0f), y1, f2_add(y0, y2)), f2_mul(il, il));
+      const f2 p = f2_mul(qs, qr);
+      f2 w = f2_mul(p, p);
+      if constexpr (MASKED) {
+        const int klo = kw + 64 * i + lane;
+        w.x = klo >= kst[n] ? w.x : 0.f;
+        w.y = klo + 32 >= kst[n] ? w.y : 0.f;
+      }
+      acc[i] = f2_fma(amp, w, acc[i]);
+    }
+  }
+}
+
+template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP, bool AA = false>
 __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, const int win,
                                             unsigned char* smem) {
   constexpr int NW = COLS * WPC;
@@ -183,7 +245,8 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   const int64_t off0 = A.off[tile];
   const int n_list = (int)(A.off[tile + 1] - off0);
   const int nb = (n_list + B - 1) / B;
-  const int lo = window_lo(A, k0, Storage<ST>::kAlign);
+  // anti-alias rows are staged whole (they carry the integral's padding)
+  const int lo = AA ? 0 : window_lo(A, k0, Storage<ST>::kAlign);
   const int rowlen = S - lo;
 
   if (tid == 0) {
@@ -245,10 +308,12 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     aa[i] = f2{1000.0f / (vl * A.in_dt), 1000.0f / (vh * A.in_dt)};
     acc[i] = f2{0.f, 0.f};
   }
-  const float bconst = -A.in_t0 / A.in_dt - (float)lo;
+  // staged position of sample index idx: idx - lo (plain) or idx + pad (AA)
+  const float shift = AA ? (float)A.aa_pad : -(float)lo;
+  const float bconst = -A.in_t0 / A.in_dt + shift;
   const f2 bb = f2_bcast(bconst);
-  const float hi_c = A.clamp_hi - (float)lo;
-  const float lo_c = -(float)lo;  // idx >= 0 (LOWC: output times before the first input)
+  const float hi_c = A.clamp_hi + shift;
+  const float lo_c = shift;  // idx >= 0 (LOWC: output times before the first input)
   const float* thr_c = thr + cl * T;
   const uint32_t raw_base = smem_addr(raw) + kRowGuard - (kMagicBits << SHIFT);
   const int kwe = kw + 64 * M;
@@ -264,6 +329,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   for (int p0 = 0; p0 < n_list && !aborted; p0 += 32) {
     // set-up of 32 list entries, one per lane
     float hs2 = 0.f, hr2 = 0.f;
+    float gxs = 0.f, gxr = 0.f, gys = 0.f, gyr = 0.f;  // AA: dip coefficients
     int ks = warp_live ? kend : 0x7fffffff;  // kend: no contribution in this window
     float tsc = 1.0f;
     const int jj = jj_next;
@@ -271,6 +337,12 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
       if (warp_live) {
         leg_h2(xc, yc, g_next, hs2, hr2);
         ks = k0 + first_valid(thr_c, nk, sqrtf(fmaxf(hs2, hr2)));
+        if constexpr (AA) {
+          gxs = (xc - g_next.x) * A.aa_dx;
+          gxr = (xc - g_next.z) * A.aa_dx;
+          gys = (yc - g_next.y) * A.aa_dy;
+          gyr = (yc - g_next.w) * A.aa_dy;
+        }
       }
       if (A.scales) tsc = __ldg(A.scales + jj);
     }
@@ -299,7 +371,28 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
       const int kb = __shfl_sync(0xffffffffu, ks, pair ? t + 1 : t);
       const bool la = ka < kwe, lb = pair && kb < kwe;
       const uint32_t rb0 = raw_base + (uint32_t)((stage * B + slot) * RP);
-      if (la && lb) {
+      if constexpr (AA) {
+        // anti-aliased sweeps take one trace at a time (three taps per sample)
+        for (int q = 0; q < (pair ? 2 : 1); ++q) {
+          const int u = t + q;
+          const int kq = q ? kb : ka;
+          if (!(q ? lb : la)) continue;
+          const float hs[1] = {__shfl_sync(0xffffffffu, hs2, u)};
+          const float hr[1] = {__shfl_sync(0xffffffffu, hr2, u)};
+          const float g0[1] = {__shfl_sync(0xffffffffu, gxs, u)};
+          const float g1[1] = {__shfl_sync(0xffffffffu, gxr, u)};
+          const float g2[1] = {__shfl_sync(0xffffffffu, gys, u)};
+          const float g3[1] = {__shfl_sync(0xffffffffu, gyr, u)};
+          const uint32_t rb[1] = {rb0 + (uint32_t)(q * RP)};
+          const int kk[1] = {kq};
+          if (kq > kw)
+            sweep_aa<M, LOWC, true, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, hi_c,
+                                       lo_c, A.aa_lmax, kw, lane);
+          else
+            sweep_aa<M, LOWC, false, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, hi_c,
+                                        lo_c, A.aa_lmax, kw, lane);
+        }
+      } else if (la && lb) {
         const float hs[2] = {__shfl_sync(0xffffffffu, hs2, t), __shfl_sync(0xffffffffu, hs2, t + 1)};
         const float hr[2] = {__shfl_sync(0xffffffffu, hr2, t), __shfl_sync(0xffffffffu, hr2, t + 1)};
         const float sc[2] = {__shfl_sync(0xffffffffu, tsc, t), __shfl_sync(0xffffffffu, tsc, t + 1)};
@@ -383,10 +476,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   }
 }
 
-template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP>
+template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP, bool AA = false>
 __global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const KArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
-  gather_tile<COLS, WPC, M, ST, WM, LOWC, OP>(A, blockIdx.x, blockIdx.y, smem);
+  gather_tile<COLS, WPC, M, ST, WM, LOWC, OP, AA>(A, blockIdx.x, blockIdx.y, smem);
 }
 
 // Persistent batched kernel: CTAs pull (class, tile, window) work items from a
@@ -419,10 +512,10 @@ __global__ void __launch_bounds__(COLS* WPC * 32, 1)
   }
 }
 
-template <int COLS, int WPC, int M, typename ST, int WM, int OP>
+template <int COLS, int WPC, int M, typename ST, int WM, int OP, bool AA = false>
 inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
-  auto kern = needs_lowclamp(p) ? pstm_gather2_kernel<COLS, WPC, M, ST, WM, true, OP>
-                                : pstm_gather2_kernel<COLS, WPC, M, ST, WM, false, OP>;
+  auto kern = needs_lowclamp(p) ? pstm_gather2_kernel<COLS, WPC, M, ST, WM, true, OP, AA>
+                                : pstm_gather2_kernel<COLS, WPC, M, ST, WM, false, OP, AA>;
   const int T = WPC * 64 * M;
   KArgs A2 = A;
   if (!ring_shape(COLS, T, p->row_stride, (int)sizeof(ST), &A2.ring_stages, &A2.ring_rows))
@@ -460,6 +553,12 @@ inline cudaError_t dispatch2_wm(const Plan* p, const KArgs& A, cudaStream_t s) {
 
 template <int COLS, int WPC, int M, int OP>
 inline cudaError_t dispatch2_st(const Plan* p, const KArgs& A, cudaStream_t s) {
+  if (p->params.antialias) {
+    if constexpr (OP == OP_FWD)
+      return launch2_one<COLS, WPC, M, float, W_OBL_SPREAD, OP, true>(p, A, s);
+    else
+      return cudaErrorNotSupported;
+  }
   switch (p->params.storage) {
     case PSTM_F32:
       return dispatch2_wm<COLS, WPC, M, float, OP>(p, A, s);

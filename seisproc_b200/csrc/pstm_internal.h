@@ -30,6 +30,7 @@ struct Plan {
   int64_t n_traces = 0;
   int n_samples = 0;
   int row_stride = 0;  // elements per staged trace row (multiple of 8)
+  int aa_pad = 0;      // anti-alias rows: integral entries before sample 0 (and after N)
   int elt_bytes = 4;
   Shape shape{};
   int tiles_il = 0, tiles_xl = 0;

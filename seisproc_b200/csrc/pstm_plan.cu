@@ -327,6 +327,87 @@ __global__ void unstage_rows_kernel(const float* acc, int64_t n_tr, int n_s, con
   for (int i = threadIdx.x; i < n_s; i += blockDim.x) out[j * n_s + i] = acc[(int64_t)jj * S + i];
 }
 
+// Anti-alias staging, one warp per sorted trace row: the samples (rounded to
+// the requested storage precision, bf16 or f16 with a per-trace scale), their
+// causal double integral in float64
+//   I1[i] = sum_{n<=i} x[n],  I2[i] = sum_{m<i} I1[m]   (i = 0..N),
+// extended with I2 = 0 before the trace and I2[N] + (i-N) I1[N-1] after it, and
+// a linear trend beta*i removed (beta = I2[N]/N) -- the triangle filter takes
+// second differences, to which linear terms contribute nothing -- stored in
+// float32 at row positions i + pad.
+__device__ __forceinline__ float quantize_sample(float x, int storage, float scale) {
+  if (storage == PSTM_BF16) return __bfloat162float(__float2bfloat16_rn(x));
+  if (storage == PSTM_F16) return __half2float(__float2half_rn(x / scale)) * scale;
+  return x;
+}
+
+__global__ void aa_integrate_kernel(const float* rows, int64_t n_tr, int n_s, int S_in, int storage,
+                                    int pad, int S_out, float* out) {
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n_tr) return;
+  const float* x = rows + row * S_in;
+  float* o = out + row * S_out;
+  float scale = 1.0f;
+  if (storage == PSTM_F16) {
+    float m = 0.f;
+    for (int i = lane; i < n_s; i += 32) m = fmaxf(m, fabsf(x[i]));
+    for (int d = 16; d > 0; d >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, d));
+    scale = m > 0.f ? m / 32768.0f : 1.0f;
+  }
+  // pass 1: totals I2[N] and I1[N-1]
+  double c1 = 0.0, c2 = 0.0;
+  for (int base = 0; base < n_s; base += 32) {
+    const int i = base + lane;
+    double v = i < n_s ? (double)quantize_sample(x[i], storage, scale) : 0.0;
+    for (int d = 1; d < 32; d <<= 1) {
+      const double u = __shfl_up_sync(0xffffffffu, v, d);
+      if (lane >= d) v += u;
+    }
+    const double i1 = v + c1;  // inclusive I1[i]
+    double e = i < n_s ? i1 : 0.0;
+    for (int d = 16; d > 0; d >>= 1) e += __shfl_xor_sync(0xffffffffu, e, d);
+    c1 = __shfl_sync(0xffffffffu, i1, 31);
+    c2 += e;
+  }
+  const double i2_end = c2, i1_last = c1;
+  const double beta = i2_end / (double)n_s;
+  // pass 2: write I2'[i] = I2[i] - beta i
+  c1 = 0.0;
+  c2 = 0.0;
+  for (int base = 0; base < n_s; base += 32) {
+    const int i = base + lane;
+    double v = i < n_s ? (double)quantize_sample(x[i], storage, scale) : 0.0;
+    for (int d = 1; d < 32; d <<= 1) {
+      const double u = __shfl_up_sync(0xffffffffu, v, d);
+      if (lane >= d) v += u;
+    }
+    const double i1 = v + c1;
+    // exclusive prefix of I1 within the chunk gives I2[i]
+    double ex = __shfl_up_sync(0xffffffffu, i1, 1);
+    if (lane == 0) ex = 0.0;
+    double acc = ex;
+    for (int d = 1; d < 32; d <<= 1) {
+      const double u = __shfl_up_sync(0xffffffffu, acc, d);
+      if (lane >= d) acc += u;
+    }
+    if (i < n_s) o[i + pad] = (float)(c2 + acc - beta * (double)i);
+    double e = i < n_s ? i1 : 0.0;
+    for (int d = 16; d > 0; d >>= 1) e += __shfl_xor_sync(0xffffffffu, e, d);
+    c1 = __shfl_sync(0xffffffffu, i1, 31);
+    c2 += e;
+  }
+  // before the trace (I2 = 0) and from I2[N] on (linear continuation)
+  for (int q = lane; q < pad; q += 32) {
+    const int i = q - pad;  // -pad .. -1
+    o[q] = (float)(-beta * (double)i);
+  }
+  for (int q = n_s + pad + lane; q < S_out; q += 32) {
+    const int i = q - pad;  // N .. 
+    o[q] = (float)(i2_end + (double)(i - n_s) * i1_last - beta * (double)i);
+  }
+}
+
 __global__ void normalize_kernel(const float* image, const float* fold, float* out, int64_t n,
                                  float min_fold, int mute) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -379,7 +460,12 @@ static pstm_status validate(const pstm_grid* g, const pstm_params* prm, const ps
   if (prm->clamp < 0 || prm->clamp > 1) return fail(PSTM_EINVAL, "unknown clamp mode");
   if (prm->storage != PSTM_F32 && prm->storage != PSTM_BF16 && prm->storage != PSTM_F16)
     return fail(PSTM_EINVAL, "storage must be F32, BF16 or F16");
-  if (prm->antialias) return fail(PSTM_ENOTSUP, "anti-alias filter is not built into this library");
+  if (prm->antialias && !(prm->aa_max_halfwidth >= 1.0 && prm->aa_max_halfwidth <= 256.0))
+    return fail(PSTM_EINVAL, "aa_max_halfwidth must be in [1, 256] samples");
+  if (prm->antialias && (!(prm->aa_dx >= 0) || !(prm->aa_dy >= 0)))
+    return fail(PSTM_EINVAL, "aa_dx/aa_dy must be non-negative");
+  if (prm->antialias && prm->weight != PSTM_WEIGHT_OBLIQUITY_SPREADING)
+    return fail(PSTM_ENOTSUP, "the anti-alias kernel is built for the obliquity x spreading weight");
   if (geo->n_traces < 0 || geo->n_traces > (int64_t)INT32_MAX)
     return fail(PSTM_EINVAL, "n_traces out of range");
   if (geo->n_traces > 0 && (!geo->source_x || !geo->source_y || !geo->receiver_x || !geo->receiver_y))
@@ -400,7 +486,8 @@ pstm_status pstm::ensure_trace_storage(Plan* p, cudaStream_t s) {
   CUDA_TRY(cudaMemsetAsync(p->traces, 0, bytes, s));
   // f16 needs a per-trace scale for its range; bf16 has float32's exponent
   // range and is stored unscaled
-  if (p->params.storage == PSTM_F16) CUDA_TRY(dalloc(p, &p->scales, p->n_traces));
+  if (p->params.storage == PSTM_F16 && !p->params.antialias)
+    CUDA_TRY(dalloc(p, &p->scales, p->n_traces));
   return PSTM_OK;
 }
 
@@ -442,6 +529,12 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
   p->n_samples = prm->n_samples;
   p->row_stride = (int)align_up(prm->n_samples, 8);
   p->elt_bytes = prm->storage == PSTM_F32 ? 4 : 2;
+  if (prm->antialias) {
+    // rows hold the trend-removed double integral I2[-pad .. N + pad] in float32
+    p->aa_pad = (int)std::ceil(prm->aa_max_halfwidth) + 2;
+    p->row_stride = (int)align_up(prm->n_samples + 1 + 2 * p->aa_pad, 8);
+    p->elt_bytes = 4;
+  }
   if (!shape_for_variant(prm->variant, g->n_xl, g->n_times, &p->shape))
     return fail(PSTM_EINVAL, "unknown kernel variant");
   p->tiles_il = (g->n_il + p->shape.tile_il - 1) / p->shape.tile_il;
@@ -624,6 +717,27 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
   pstm_status st = ensure_trace_storage(p, s);
   if (st != PSTM_OK) return st;
   const int thr = 256;
+  if (p->params.antialias) {
+    // plain float32 rows into the adjoint accumulator (free until demigration),
+    // then one warp per row integrates into the staged rows
+    const int S_in = (int)align_up(n_s, 8);
+    if (!p->accum) CUDA_TRY(dalloc(p, &p->accum, (size_t)n * p->row_stride));
+    dim3 tb(32, 8);
+    dim3 tg((unsigned)((n + 31) / 32), (unsigned)((n_s + 31) / 32));
+    if (trace_major)
+      stage_rows_kernel<float><<<(unsigned)n, 256, 0, s>>>(traces, n, n_s, p->perm, nullptr, S_in,
+                                                           p->accum);
+    else
+      stage_transpose_kernel<float><<<tg, tb, 0, s>>>(traces, n, n_s, p->inv_perm, nullptr, S_in,
+                                                      p->accum);
+    LAUNCH_CHECK("stage kernel");
+    aa_integrate_kernel<<<(unsigned)((n + 7) / 8), 256, 0, s>>>(
+        p->accum, n, n_s, S_in, p->params.storage, p->aa_pad, p->row_stride,
+        reinterpret_cast<float*>(p->traces));
+    LAUNCH_CHECK("aa_integrate_kernel");
+    p->traces_loaded = true;
+    return PSTM_OK;
+  }
   if (p->params.storage == PSTM_F16) {
     const float target = 32768.0f;
     maxabs_kernel<<<(unsigned)((n + thr - 1) / thr), thr, 0, s>>>(traces, n, n_s, trace_major,
@@ -701,6 +815,8 @@ pstm_status pstm_demigrate(pstm_plan* plan, const float* image, const float* vel
                            int64_t vsc, float* traces_out, int32_t trace_major, void* stream) {
   if (!plan || !image || !traces_out) return fail(PSTM_EINVAL, "null argument");
   Plan* p = reinterpret_cast<Plan*>(plan);
+  if (p->params.antialias)
+    return fail(PSTM_ENOTSUP, "demigration is built for the plain (non-anti-aliased) operator");
   pstm_status st = check_velocity_args(vel, vst, vsc);
   if (st != PSTM_OK) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -732,8 +848,9 @@ pstm_status pstm_velocity_gradient(pstm_plan* plan, const float* grad_image, con
   if (!plan || !grad_image || !grad_v) return fail(PSTM_EINVAL, "null argument");
   Plan* p = reinterpret_cast<Plan*>(plan);
   if (!p->traces_loaded) return fail(PSTM_EINVAL, "no traces loaded into the plan");
-  if (p->params.weight != PSTM_WEIGHT_OBLIQUITY_SPREADING)
-    return fail(PSTM_ENOTSUP, "velocity gradient is built for the obliquity x spreading weight");
+  if (p->params.weight != PSTM_WEIGHT_OBLIQUITY_SPREADING || p->params.antialias)
+    return fail(PSTM_ENOTSUP, "velocity gradient is built for the plain obliquity x spreading "
+                              "operator");
   pstm_status st = check_velocity_args(vel, vst, vsc);
   if (st != PSTM_OK) return st;
   std::string why;

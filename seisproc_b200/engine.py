@@ -97,9 +97,15 @@ class MigrationEngine:
         use_time_dependent_aperture: bool = False,
         velocity_model=None,
         kernel_backend=None,
+        antialias: bool = False,
+        aa_max_halfwidth: float = 32.0,
     ) -> Tuple[np.ndarray, np.ndarray]:
         """Full Kirchhoff migration of one bin; returns (image, fold) as
-        (n_times, n_il, n_xl) float32 numpy arrays."""
+        (n_times, n_il, n_xl) float32 numpy arrays.
+
+        ``antialias`` applies the causal-integrated triangle filter whose
+        half-width follows the operator dip times the bin spacing (capped at
+        ``aa_max_halfwidth`` input samples)."""
         t_start = time.perf_counter()
         require_cuda(kernel_backend if kernel_backend is not None else self.kernel_backend)
         traces = np.asarray(traces)
@@ -130,7 +136,9 @@ class MigrationEngine:
                             max_angle_deg=max_angle_deg,
                             time_dependent_aperture=use_time_dependent_aperture,
                             storage=self.storage, variant=self.variant,
-                            kernel_backend=kernel_backend or self.kernel_backend)
+                            kernel_backend=kernel_backend or self.kernel_backend,
+                            antialias=antialias, aa_dx=il_spacing, aa_dy=xl_spacing,
+                            aa_max_halfwidth=aa_max_halfwidth)
             try:
                 if progress_callback:
                     progress_callback(0.1, "Running Kirchhoff migration...")

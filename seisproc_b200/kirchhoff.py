@@ -75,7 +75,8 @@ class PSTMPlan:
                  in_t0_ms: float, in_dt_ms: float, max_aperture_m: float, max_angle_deg: float,
                  time_dependent_aperture: bool = False, weight: str = "obliquity_spreading",
                  clamp: str = "full", storage: str = "f32", variant: int = 0,
-                 kernel_backend=None):
+                 kernel_backend=None, antialias: bool = False, aa_dx: float = 0.0,
+                 aa_dy: float = 0.0, aa_max_halfwidth: float = 32.0):
         require_cuda(kernel_backend)
         self._lib = _lib.lib()
         self._handle = C.c_void_p(None)
@@ -101,7 +102,8 @@ class PSTMPlan:
                               t0_ms, dt_ms)
         self.params = _lib.Params(n_samples, in_t0_ms, in_dt_ms, max_aperture_m, max_angle_deg,
                                   int(bool(time_dependent_aperture)), WEIGHTS[weight],
-                                  CLAMPS[clamp], STORAGES[storage], 0, 0.0, 0.0, 0.0,
+                                  CLAMPS[clamp], STORAGES[storage], int(bool(antialias)),
+                                  float(aa_dx), float(aa_dy), float(aa_max_halfwidth),
                                   int(variant))
         geo = _lib.Geometry(n_tr, _lib.PSTM_F64 if dt == torch.float64 else _lib.PSTM_F32,
                             *[c.data_ptr() for c in coords])

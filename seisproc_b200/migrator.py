@@ -164,7 +164,8 @@ class KirchhoffMigrator(BaseMigrator):
 
     def __init__(self, velocity: VelocityModel, config: MigrationConfig,
                  device: Optional[torch.device] = None, use_traveltime_lut: bool = True,
-                 kernel_backend=None, storage: str = "f32", variant: int = 0):
+                 kernel_backend=None, storage: str = "f32", variant: int = 0,
+                 antialias: bool = False, aa_max_halfwidth: float = 32.0):
         self.velocity = velocity
         require_cuda(kernel_backend)
         self.device = torch.device(device) if device is not None else \
@@ -175,6 +176,10 @@ class KirchhoffMigrator(BaseMigrator):
         self.kernel_backend = kernel_backend
         self.storage = storage
         self.variant = variant
+        # the reference migrator never applies its anti-alias filter; it is an
+        # explicit opt-in here (weight FULL only)
+        self.antialias = antialias
+        self.aa_max_halfwidth = aa_max_halfwidth
         super().__init__(velocity, config)
 
     def _validate_inputs(self):
@@ -227,7 +232,9 @@ class KirchhoffMigrator(BaseMigrator):
                 max_aperture_m=self.config.max_aperture_m,
                 max_angle_deg=self.config.max_angle_deg,
                 weight=_WEIGHT_OF_MODE[self.config.weight_mode], clamp="migrator",
-                storage=self.storage, variant=self.variant, kernel_backend=self.kernel_backend)
+                storage=self.storage, variant=self.variant, kernel_backend=self.kernel_backend,
+                antialias=self.antialias, aa_dx=g.d_inline, aa_dy=g.d_xline,
+                aa_max_halfwidth=self.aa_max_halfwidth)
             try:
                 v = torch.from_numpy(np.ascontiguousarray(self._velocity_grid())).to(self.device)
                 tr = torch.from_numpy(np.ascontiguousarray(traces, dtype=np.float32))
