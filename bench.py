@@ -7,7 +7,14 @@ m/s with a +-5 % lateral sinusoid, output 200 x 200 x 1000 at 25 m, 1000 m
 aperture, 60 deg angle.  Synthetic, seeded.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|bf16|f16]
+                  [--antialias] [--utm]
   python bench.py --impl reference ...   (CPU port of the reference kernel)
+  python bench.py --config batched | lsq
+
+``--antialias --utm --storage bf16|f16`` is the anti-aliased workload with
+traces stored in 16 bits and world coordinates offset by a UTM origin.  Every
+run quotes ``error_vs_fp64``: the rel-L2 of its image against the FP64 oracle on
+a small centred crop of columns (``--err-crop``).
 
 One JSON line on rank 0.  ``value`` = pairs / device time of one step with the
 inputs resident in HBM (stage traces + fold + forward migration; the geometry
@@ -106,10 +113,61 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+UTM_ORIGIN = (5.0e5, 6.0e6)
+
+
 def make_workload(device, rank: int, args):
     from seisproc_b200 import synthetic
     return synthetic.survey_3d(n_traces=args.traces, seed=2025 + rank, device=device,
-                               n_samples=args.samples, n_il=args.grid, n_xl=args.grid)
+                               n_samples=args.samples, n_il=args.grid, n_xl=args.grid,
+                               utm_origin=UTM_ORIGIN if getattr(args, "utm", False) else (0.0, 0.0))
+
+
+def workload_name(args) -> str:
+    if (args.storage == "f32" and args.traces == 500_000 and not args.antialias
+            and not args.utm and args.samples == 1000 and args.grid == 200):
+        return ("3D PSTM plain FP32 (500k traces x 1000 samples, 200x200x1000 output, "
+                "V_rms(t0,x,y), A=1000 m, 60 deg)")
+    extra = []
+    if args.antialias:
+        extra.append(f"triangle anti-alias (half-width <= {args.aa_lmax:g} samples)")
+    if args.utm:
+        extra.append(f"UTM origin ({UTM_ORIGIN[0]:.0e}, {UTM_ORIGIN[1]:.0e}) m")
+    return (f"3D PSTM {args.storage} storage{', ' if extra else ''}{', '.join(extra)} "
+            f"({args.traces} traces x {args.samples} samples, {args.grid}x{args.grid}x"
+            f"{args.samples} output, V_rms(t0,x,y), A=1000 m, 60 deg)")
+
+
+def crop_traces(s, cols):
+    """Traces with both legs inside the aperture of some column of the crop."""
+    il = cols // s.n_xl
+    xl = cols % s.n_xl
+    cx = s.origin_x + il * s.il_spacing
+    cy = s.origin_y + xl * s.xl_spacing
+    mx, my = cx.mean(), cy.mean()
+    r = s.max_aperture_m + float(np.hypot(cx - mx, cy - my).max()) + 1.0
+    keep = ((np.hypot(s.source_x - mx, s.source_y - my) <= r)
+            & (np.hypot(s.receiver_x - mx, s.receiver_y - my) <= r))
+    return np.nonzero(keep)[0], cx, cy
+
+
+def run_fp64_crop(s, cols, antialias: bool, l_max: float):
+    """FP64 oracle image of the crop columns (checker and, for the anti-alias
+    workload, the CPU baseline: the reference has no anti-aliased migration)."""
+    from oracle import pstm_fp64 as O
+    idx, cx, cy = crop_traces(s, cols)
+    tr = s.traces[:, torch.from_numpy(idx).to(s.traces.device)].cpu().numpy()
+    n_t = s.n_times
+    t_ms = (np.arange(n_t, dtype=np.float32) * np.float32(s.dt_ms)).astype(np.float64)
+    vel = s.vrms.reshape(n_t, -1)[:, cols]
+    ox, oy = s.origin_x, s.origin_y
+    t0 = time.perf_counter()
+    img, fold = O.migrate_fp64(tr, s.source_x[idx] - ox, s.source_y[idx] - oy,
+                               s.receiver_x[idx] - ox, s.receiver_y[idx] - oy, cx - ox, cy - oy,
+                               t_ms, vel, s.dt_ms, 0.0, s.max_aperture_m, s.max_angle_deg,
+                               antialias=antialias, dx_out=s.il_spacing, dy_out=s.xl_spacing,
+                               l_max=l_max)
+    return img, fold, time.perf_counter() - t0, int(idx.size)
 
 
 def cpu_crop_columns(s, side: int):
@@ -145,6 +203,11 @@ def bench_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if args.antialias:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference migrators have no anti-alias filter on this path"}),
+              flush=True)
+        return
     s = make_workload("cpu" if not torch.cuda.is_available() else "cuda", 0, args)
     from oracle import pstm_fp64 as O
     cols = cpu_crop_columns(s, args.crop)
@@ -170,8 +233,7 @@ def bench_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": "3D PSTM plain FP32 (500k traces x 1000 samples, 200x200x1000 "
-                               "output, V_rms(t0,x,y), A=1000 m, 60 deg)",
+        "config": {"workload": workload_name(args), "storage": "f32",
                    "traces": s.n_traces, "samples": s.n_samples},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "Gpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -209,7 +271,9 @@ def bench_ours(args):
                     origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
                     xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
                     in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
-                    max_angle_deg=s.max_angle_deg, storage=args.storage, variant=args.variant)
+                    max_angle_deg=s.max_angle_deg, storage=args.storage, variant=args.variant,
+                    antialias=args.antialias, aa_dx=s.il_spacing, aa_dy=s.xl_spacing,
+                    aa_max_halfwidth=args.aa_lmax)
     torch.cuda.synchronize()
     t_plan = time.perf_counter() - t_plan
     traces = s.traces
@@ -282,7 +346,8 @@ def bench_ours(args):
         kw = dict(origin_x=s.origin_x, origin_y=s.origin_y, il_spacing=s.il_spacing,
                   xl_spacing=s.xl_spacing, azimuth_deg=0.0, n_il=s.n_il, n_xl=s.n_xl,
                   dt_ms=s.dt_ms, t_min_ms=0.0, n_times=n_t, max_aperture_m=s.max_aperture_m,
-                  max_angle_deg=s.max_angle_deg, normalize=True)
+                  max_angle_deg=s.max_angle_deg, normalize=True, antialias=args.antialias,
+                  aa_max_halfwidth=args.aa_lmax)
         run = lambda: eng.migrate_bin_full(host_tr.numpy(), *[h.numpy() for h in host_c],
                                            velocity_model=host_v.numpy(), **kw)
         run()
@@ -312,40 +377,64 @@ def bench_ours(args):
         pk = peaks()
         clocks = clk.summary()
         fwd_avg = statistics.mean(fwd_ms)
-        peak_pairs = 148 * MUFU_PER_SM_CLK / RSQRT_PER_PAIR * pk["sm_max_mhz"] * 1e6 / 1e12
+        mufu_per_pair = RSQRT_PER_PAIR + (1 if args.antialias else 0)
+        peak_pairs = 148 * MUFU_PER_SM_CLK / mufu_per_pair * pk["sm_max_mhz"] * 1e6 / 1e12
         achieved = pairs / (fwd_avg * 1e-3) / 1e12
-        traffic = DRAM_BYTES_PER_LIST_ENTRY * plan.stats()["list_entries"]
+        plain_f32 = args.storage == "f32" and not args.antialias
+        traffic = DRAM_BYTES_PER_LIST_ENTRY * plan.stats()["list_entries"] if plain_f32 else None
         roof = {"bound": "mufu", "achieved": achieved, "peak": peak_pairs, "unit": "Tpairs/s",
                 "frac": achieved / peak_pairs, "traffic": traffic,
+                "mufu_per_pair": mufu_per_pair,
                 "traffic_note": "DRAM bytes per launch scaled from the ncu capture of the "
-                                "100k-trace case by list entries",
-                "hbm_achieved_gbs": traffic / (fwd_avg * 1e-3) / 1e9,
+                                "100k-trace case by list entries" if plain_f32 else
+                                "not captured for this storage/filter",
+                "hbm_achieved_gbs": traffic / (fwd_avg * 1e-3) / 1e9 if traffic else None,
                 "hbm_peak_gbs": pk["hbm_gbs"],
                 "peak_source": f"{pk['source']} sm_max_mhz {pk['sm_max_mhz']}",
-                "kernel": "pstm_gather_kernel (forward)", "kernel_ms": fwd_avg,
+                "kernel": "pstm_gather2_kernel (forward)", "kernel_ms": fwd_avg,
                 "stage_ms": statistics.mean(stage_ms), "fold_ms": statistics.mean(fold_ms)}
         cb = None
+        err = None
         if world == 1 and not args.no_cpu:
-            cols = cpu_crop_columns(s, args.crop)
-            fold_cols = float(f.reshape(n_t, -1)[:, torch.from_numpy(cols).to(dev)].double().sum())
-            cb = run_cpu_port(s, cols, fold_cols)
-            cb.pop("seconds", None)
+            img_cols = image.reshape(n_t, -1)
+            fold_cols_t = f.reshape(n_t, -1)
+            # error of this result against the FP64 oracle on a small crop
+            ecols = cpu_crop_columns(s, args.err_crop)
+            eidx = torch.from_numpy(ecols).to(dev)
+            oi, of, o_sec, o_tr = run_fp64_crop(s, ecols, args.antialias, args.aa_lmax)
+            gi = img_cols[:, eidx].double().cpu().numpy()
+            gf = fold_cols_t[:, eidx].double().cpu().numpy()
+            err = {"rel_l2": float(np.linalg.norm(gi - oi) / max(np.linalg.norm(oi), 1e-300)),
+                   "fold_mismatch": float(np.abs(gf - of).sum()),
+                   "columns": int(ecols.size), "traces_in_crop": o_tr,
+                   "oracle": "FP64 restatement" + (" with anti-alias" if args.antialias else ""),
+                   "storage": args.storage}
+            if args.antialias:
+                # the reference has no anti-aliased migration: the FP64 oracle
+                # run above is the CPU baseline
+                pc = float(gf.sum())
+                cb = {"value": pc / o_sec / 1e9, "unit": "Gpairs/s", "cores": 1, "kind": "port",
+                      "sample": f"centred {args.err_crop}x{args.err_crop}-column crop x {n_t} "
+                                f"samples, {o_tr} traces in its aperture, {pc:.3e} pairs; FP64 "
+                                "numpy restatement with anti-alias (the reference has none)"}
+            else:
+                cols = cpu_crop_columns(s, args.crop)
+                fold_cols = float(fold_cols_t[:, torch.from_numpy(cols).to(dev)].double().sum())
+                cb = run_cpu_port(s, cols, fold_cols)
+                cb.pop("seconds", None)
         result = {
             "metric": "PSTM Gpairs/s (out-sample x trace)", "value": value, "unit": "Gpairs/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": args.storage, "data": "synthetic",
-            "config": {"workload": "3D PSTM plain FP32 (500k traces x 1000 samples, 200x200x1000 "
-                                   "output, V_rms(t0,x,y), A=1000 m, 60 deg)"
-                       if args.storage == "f32" and args.traces == 500_000 else
-                       f"3D PSTM {args.storage} storage ({args.traces} traces x {args.samples} "
-                       f"samples, {args.grid}x{args.grid}x{args.samples} output)",
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(args), "storage": args.storage,
+                       "antialias": bool(args.antialias),
                        "traces_per_gpu": s.n_traces, "pairs_per_step_per_gpu": pairs,
                        "plan": plan.stats(), "plan_build_s": t_plan, "datagen_s": t_gen,
                        "l2": "inputs (traces) larger than L2; no flush",
                        "parallelism": f"output-survey shards, {world} rank(s), no collective"},
             "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clocks,
+            "clocks": clocks, "error_vs_fp64": err,
         }
         print(json.dumps(result), flush=True)
     plan.close()
@@ -494,6 +583,13 @@ def main():
     ap.add_argument("--crop", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--err-crop", type=int, default=2,
+                    help="side of the column crop checked against the FP64 oracle")
+    ap.add_argument("--antialias", action="store_true",
+                    help="triangle anti-alias filter (half-width from the operator dip)")
+    ap.add_argument("--aa-lmax", type=float, default=32.0)
+    ap.add_argument("--utm", action="store_true",
+                    help="world coordinates offset by a UTM origin (5e5, 6e6) m")
     ap.add_argument("--config", default="3d", choices=["3d", "batched", "lsq"])
     args = ap.parse_args()
     if args.config == "batched" and args.impl == "ours":

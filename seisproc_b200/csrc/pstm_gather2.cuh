@@ -83,18 +83,23 @@ __device__ __forceinline__ float lds_elem<__half>(uint32_t addr) {
 // distances hs2[n], hr2[n], the shared-memory address of its staged row minus
 // the bit pattern of 2^23 (so the index's float bits address the sample), its
 // first contributing sample kst[n] (samples before it get weight 0 when
-// MASKED) and, for f16 storage, its scale.
+// MASKED) and, for f16 storage, its scale.  A MASKED sweep starts at group g0,
+// the first 64-sample group holding a contributing sample of any of its traces
+// (warp-uniform, so the skipped groups cost one uniform branch each).
 template <int M, typename ST, int WM, bool LOWC, bool MASKED, int OP, int NTR>
 __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], const f2 (&aa)[M],
                                              const float (&hs2)[NTR], const float (&hr2)[NTR],
                                              const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
                                              const float (&sc)[NTR], f2 bb, float hi_c,
-                                             float lo_c, int kw, int lane) {
+                                             float lo_c, int kw, int lane, int g0) {
   constexpr int ES = (int)sizeof(ST);
   constexpr int SHIFT = ES == 4 ? 2 : 1;
   const f2 magic2 = f2_bcast(kMagic);
 #pragma unroll
   for (int i = 0; i < M; ++i) {
+    if constexpr (MASKED) {
+      if (i < g0) continue;
+    }
 #pragma unroll
     for (int n = 0; n < NTR; ++n) {
       const f2 hs2b = f2_bcast(hs2[n]), hr2b = f2_bcast(hr2[n]);
@@ -169,7 +174,7 @@ __device__ __forceinline__ void sweep_aa(f2 (&acc)[M], const f2 (&zz)[M], const 
                                          const float (&gys)[NTR], const float (&gyr)[NTR],
                                          const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
                                          f2 bb, float hi_c, float lo_c, float lmax, int kw,
-                                         int lane) {
+                                         int lane, int g0) {
   const f2 magic2 = f2_bcast(kMagic);
   auto tap = [&](f2 pos, uint32_t base) {
     const f2 tm = f2_add_rm(pos, magic2);
@@ -182,6 +187,9 @@ __device__ __forceinline__ void sweep_aa(f2 (&acc)[M], const f2 (&zz)[M], const 
   };
 #pragma unroll
   for (int i = 0; i < M; ++i) {
+    if constexpr (MASKED) {
+      if (i < g0) continue;
+    }
 #pragma unroll
     for (int n = 0; n < NTR; ++n) {
       const f2 rrs = f2_add(f2_bcast(hs2[n]), zz[i]);
@@ -387,10 +395,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
           const int kk[1] = {kq};
           if (kq > kw)
             sweep_aa<M, LOWC, true, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, hi_c,
-                                       lo_c, A.aa_lmax, kw, lane);
+                                       lo_c, A.aa_lmax, kw, lane, (kq - kw) >> 6);
           else
             sweep_aa<M, LOWC, false, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, hi_c,
-                                        lo_c, A.aa_lmax, kw, lane);
+                                        lo_c, A.aa_lmax, kw, lane, 0);
         }
       } else if (la && lb) {
         const float hs[2] = {__shfl_sync(0xffffffffu, hs2, t), __shfl_sync(0xffffffffu, hs2, t + 1)};
@@ -400,10 +408,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const int kk[2] = {ka, kb};
         if (ka > kw || kb > kw)
           sweep_traces<M, ST, WM, LOWC, true, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
-                                                      lo_c, kw, lane);
+                                                      lo_c, kw, lane, (min(ka, kb) - kw) >> 6);
         else
           sweep_traces<M, ST, WM, LOWC, false, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
-                                                       lo_c, kw, lane);
+                                                       lo_c, kw, lane, 0);
       } else if (la || lb) {
         const int u = la ? t : t + 1;
         const float hs[1] = {__shfl_sync(0xffffffffu, hs2, u)};
@@ -413,10 +421,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const int kk[1] = {la ? ka : kb};
         if (kk[0] > kw)
           sweep_traces<M, ST, WM, LOWC, true, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
-                                                      lo_c, kw, lane);
+                                                      lo_c, kw, lane, (kk[0] - kw) >> 6);
         else
           sweep_traces<M, ST, WM, LOWC, false, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
-                                                       lo_c, kw, lane);
+                                                       lo_c, kw, lane, 0);
       }
       const int adv = pair ? 2 : 1;
       t += adv;
