@@ -296,7 +296,12 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     for (int b = 0; b < min(nb, kStages); ++b) issue(b);
 
   // -------------------------------------------------------------- consumers
-  const int cl = warp / WPC, ts = warp % WPC;
+  // Warp -> (column, time segment).  The scheduler of warp w is w % 4; the
+  // shallow segments mask out more samples than the deep ones, so every
+  // scheduler gets warps of all segments (when there are enough warps).
+  constexpr bool kMix = NW % (4 * WPC) == 0;
+  const int cl = kMix ? (warp & 3) + 4 * (warp / (4 * WPC)) : warp / WPC;
+  const int ts = kMix ? (warp >> 2) % WPC : (warp + (WPC / 2) * (warp / WPC)) % WPC;
   int il, xl;
   const bool col_ok = tile_column(A, tile, cl, il, xl);
   const int c = col_ok ? il * A.n_xl + xl : 0;
@@ -338,13 +343,14 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     // set-up of 32 list entries, one per lane
     float hs2 = 0.f, hr2 = 0.f;
     float gxs = 0.f, gxr = 0.f, gys = 0.f, gyr = 0.f;  // AA: dip coefficients
-    int ks = warp_live ? kend : 0x7fffffff;  // kend: no contribution in this window
+    int ks = 0x7fffffff;  // no contribution in this window
     float tsc = 1.0f;
     const int jj = jj_next;
     if (p0 + lane < n_list) {
       if (warp_live) {
         leg_h2(xc, yc, g_next, hs2, hr2);
-        ks = k0 + first_valid(thr_c, nk, sqrtf(fmaxf(hs2, hr2)));
+        const int fv = first_valid(thr_c, nk, sqrtf(fmaxf(hs2, hr2)));
+        if (fv < nk) ks = k0 + fv;
         if constexpr (AA) {
           gxs = (xc - g_next.x) * A.aa_dx;
           gxr = (xc - g_next.z) * A.aa_dx;

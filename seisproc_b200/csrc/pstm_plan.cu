@@ -8,6 +8,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "pstm_common.cuh"
 #include "pstm_internal.h"
@@ -236,6 +237,30 @@ __global__ void __launch_bounds__(256) tile_fill_kernel(TileGeom tg, CellGrid cg
   }
 }
 
+// Sort key of a list entry: the larger squared leg distance from the tile
+// centre (non-negative float, so its bits order like the value).  Sorting a
+// tile's list by it lines up traces whose first contributing output sample is
+// close, so the two traces a warp sweeps together mask out few samples.
+__global__ void __launch_bounds__(256) tile_key_kernel(TileGeom tg, const float4* geo,
+                                                       const int64_t* off, int tile0,
+                                                       const int* list, int64_t base,
+                                                       uint32_t* keys, int* seg) {
+  const int tile = tile0 + blockIdx.x;
+  float cx, cy, r2, rad;
+  tile_disc(tg, tile, cx, cy, r2, rad);
+  const int64_t a = off[tile], b = off[tile + 1];
+  if (threadIdx.x == 0) {
+    seg[blockIdx.x] = (int)(a - base);
+    seg[blockIdx.x + 1] = (int)(b - base);
+  }
+  for (int64_t j = a + threadIdx.x; j < b; j += blockDim.x) {
+    const float4 g = geo[list[j]];
+    const float ds = (g.x - cx) * (g.x - cx) + (g.y - cy) * (g.y - cy);
+    const float dr = (g.z - cx) * (g.z - cx) + (g.w - cy) * (g.w - cy);
+    keys[j - base] = __float_as_uint(fmaxf(ds, dr));
+  }
+}
+
 // --------------------------------------------------------- trace staging ---
 
 __global__ void maxabs_kernel(const float* tr, int64_t n_tr, int n_s, int trace_major,
@@ -430,6 +455,69 @@ static cudaError_t dalloc(Plan* p, T** ptr, size_t count) {
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(ptr), bytes);
   if (e == cudaSuccess) p->bytes += (int64_t)bytes;
   return e;
+}
+
+// Orders every tile's trace list by tile_key_kernel's key (stable, so the
+// order is reproducible), in chunks of whole tiles that bound the temporaries.
+static cudaError_t sort_tile_lists(Plan* p, const TileGeom& tg, cudaStream_t s) {
+  const int64_t n_tiles = p->n_tiles;
+  std::vector<int64_t> off(n_tiles + 1);
+  cudaError_t e = cudaMemcpyAsync(off.data(), p->tile_off, off.size() * sizeof(int64_t),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  constexpr int64_t kChunk = int64_t(1) << 24;
+  int64_t cap = 0, longest = 0;
+  for (int64_t t = 0; t < n_tiles; ++t) longest = std::max(longest, off[t + 1] - off[t]);
+  cap = std::min(off[n_tiles], std::max(kChunk, longest));
+  if (cap <= 1 || cap > INT32_MAX) return cudaSuccess;  // order is only a speed hint
+  constexpr int64_t kMaxSegs = 65535;                      // tiles per key launch
+  uint32_t *kin = nullptr, *kout = nullptr;
+  int *vout = nullptr, *seg = nullptr;
+  void* tmp = nullptr;
+  size_t tmp_bytes = 0;
+  struct Free {
+    void** ptrs[5];
+    ~Free() {
+      for (auto pp : ptrs)
+        if (*pp) cudaFree(*pp);
+    }
+  } fr{{(void**)&kin, (void**)&kout, (void**)&vout, (void**)&seg, &tmp}};
+  if ((e = cudaMalloc(&kin, cap * sizeof(uint32_t))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&kout, cap * sizeof(uint32_t))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&vout, cap * sizeof(int))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&seg, (kMaxSegs + 1) * sizeof(int))) != cudaSuccess) return e;
+  for (int64_t ta = 0; ta < n_tiles;) {
+    int64_t tb = ta + 1;
+    while (tb < n_tiles && tb - ta < kMaxSegs && off[tb + 1] - off[ta] <= cap) ++tb;
+    const int64_t base = off[ta], items = off[tb] - base;
+    const int nseg = (int)(tb - ta);
+    if (items > 1) {
+      tile_key_kernel<<<nseg, 256, 0, s>>>(tg, p->geo, p->tile_off, (int)ta, p->tile_list, base,
+                                           kin, seg);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      size_t need = 0;
+      e = cub::DeviceSegmentedSort::StableSortPairs(nullptr, need, kin, kout, p->tile_list + base,
+                                                    vout, (int)items, nseg, seg, seg + 1, s);
+      if (e != cudaSuccess) return e;
+      if (need > tmp_bytes) {
+        cudaFree(tmp);
+        tmp = nullptr;
+        if ((e = cudaMalloc(&tmp, need)) != cudaSuccess) return e;
+        tmp_bytes = need;
+      }
+      e = cub::DeviceSegmentedSort::StableSortPairs(tmp, tmp_bytes, kin, kout,
+                                                    p->tile_list + base, vout, (int)items, nseg,
+                                                    seg, seg + 1, s);
+      if (e != cudaSuccess) return e;
+      e = cudaMemcpyAsync(p->tile_list + base, vout, items * sizeof(int),
+                          cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return e;
+      count_launch();
+    }
+    ta = tb;
+  }
+  return cudaStreamSynchronize(s);
 }
 
 static void free_plan(Plan* p) {
@@ -676,6 +764,7 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
     tile_fill_kernel<<<(unsigned)p->n_tiles, 256, 0, s>>>(tg, cg, cell_start, p->geo, p->tile_off,
                                                           p->tile_list);
     LAUNCH_CHECK("tile_fill_kernel");
+    CUDA_TRY(sort_tile_lists(p, tg, s));
   }
   CUDA_TRY(cudaStreamSynchronize(s));
   guard.keep = true;
