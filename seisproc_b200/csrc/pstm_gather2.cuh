@@ -57,6 +57,13 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
+// Forward sweeps with a weight that is a power of p = q_s q_r (or none) run on
+// traveltimes pre-scaled by the index scale a = 1000 / (V dt): the per-sample
+// tables hold a^2 (z^2 + eps) and a^2 and the power of a comes back in the
+// epilogue, which saves an FP32 op per sample pair.
+template <int OP, int WM>
+constexpr bool kPrescaled = OP == OP_FWD && (WM == W_OBL_SPREAD || WM == W_OBL || WM == W_NONE);
+
 template <typename ST>
 __device__ __forceinline__ float lds_elem(uint32_t addr);
 template <>
@@ -103,12 +110,23 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
 #pragma unroll
     for (int n = 0; n < NTR; ++n) {
       const f2 hs2b = f2_bcast(hs2[n]), hr2b = f2_bcast(hr2[n]);
-      const f2 rrs = f2_add(hs2b, zz[i]);
-      const f2 rrr = f2_add(hr2b, zz[i]);
-      const f2 qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
-      const f2 qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
-      const f2 sum = f2_fma(rrr, qr, f2_mul(rrs, qs));
-      f2 id = f2_fma(sum, aa[i], bb);
+      f2 rrs, rrr, qs, qr, id;
+      if constexpr (kPrescaled<OP, WM>) {
+        // zz = a^2 (z^2 + eps), aa = a^2: rr' = a^2 rr, q' = q / a, and
+        // rr'_s q'_s + rr'_r q'_r = a (r_s + r_r), the index less its offset
+        rrs = f2_fma(hs2b, aa[i], zz[i]);
+        rrr = f2_fma(hr2b, aa[i], zz[i]);
+        qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
+        qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
+        id = f2_fma(rrr, qr, f2_fma(rrs, qs, bb));
+      } else {
+        rrs = f2_add(hs2b, zz[i]);
+        rrr = f2_add(hr2b, zz[i]);
+        qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
+        qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
+        const f2 sum = f2_fma(rrr, qr, f2_mul(rrs, qs));
+        id = f2_fma(sum, aa[i], bb);
+      }
       const f2 id_raw = id;
       id.x = fminf(id.x, hi_c);
       id.y = fminf(id.y, hi_c);
@@ -125,6 +143,21 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
       const f2 dx = f2_sub(x1, x0);
       const f2 amp = f2_fma(fr, dx, x0);
       const f2 p = f2_mul(qs, qr);
+      if constexpr (kPrescaled<OP, WM>) {
+        // weight p^2 (obliquity x spreading; the a^4 z^2 factor comes in the
+        // epilogue), p (obliquity) or 1; formed while the taps load
+        f2 w = p;
+        if constexpr (WM == W_OBL_SPREAD) w = f2_mul(p, p);
+        if constexpr (WM == W_NONE) w = f2_bcast(1.0f);
+        if constexpr (std::is_same<ST, __half>::value) w = f2_mul(w, f2_bcast(sc[n]));
+        if constexpr (MASKED) {
+          const int klo = kw + 64 * i + lane;
+          w.x = klo >= kst[n] ? w.x : 0.f;
+          w.y = klo + 32 >= kst[n] ? w.y : 0.f;
+        }
+        acc[i] = f2_fma(amp, w, acc[i]);
+        continue;
+      }
       f2 w;
       if constexpr (WM == W_OBL_SPREAD) {
         w = f2_mul(p, p);
@@ -319,6 +352,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     const float zh = depth_of(vh, out_time_ms(kh, A.out_dt, A.out_t0));
     zz[i] = f2{fmaf(zl, zl, kRadicandFloor), fmaf(zh, zh, kRadicandFloor)};
     aa[i] = f2{1000.0f / (vl * A.in_dt), 1000.0f / (vh * A.in_dt)};
+    if constexpr (!AA && kPrescaled<OP, WM>) {
+      aa[i] = f2_mul(aa[i], aa[i]);
+      zz[i] = f2_mul(zz[i], aa[i]);
+    }
     acc[i] = f2{0.f, 0.f};
   }
   // staged position of sample index idx: idx - lo (plain) or idx + pad (AA)
@@ -480,6 +517,13 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
       const float zh = depth_of(vh, out_time_ms(kh, A.out_dt, A.out_t0));
       fl = zl * zl;
       fh = zh * zh;
+      if constexpr (!AA && kPrescaled<OP, WM>) {
+        // the pre-scaled weight p' = p / a^2: multiply by a^4 (p^2) or a^2 (p)
+        const float al = 1000.0f / (vl * A.in_dt), ah = 1000.0f / (vh * A.in_dt);
+        const float al2 = al * al, ah2 = ah * ah;
+        fl *= WM == W_OBL_SPREAD ? al2 * al2 : al2;
+        fh *= WM == W_OBL_SPREAD ? ah2 * ah2 : ah2;
+      }
       if (OP == OP_VGRAD) {
         fl = klo < A.n_times ? fl / vl * A.in_img[(long long)klo * n_c + c] : 0.f;
         fh = khi < A.n_times ? fh / vh * A.in_img[(long long)khi * n_c + c] : 0.f;
