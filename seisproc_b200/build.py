@@ -22,7 +22,7 @@ SOURCES = [
     "pstm_plan.cu",
     "pstm_migrate.cu",
     "pstm_gather_fwd.cu",
-    "pstm_gather_adj.cu",
+    "pstm_adjoint.cu",
     "pstm_gather_vgrad.cu",
     "pstm_noalloc.cu",
     "pstm_batch.cu",

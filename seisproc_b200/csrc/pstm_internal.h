@@ -49,6 +49,13 @@ struct Plan {
   void* traces = nullptr;        // n_traces x row_stride, storage dtype
   float* scales = nullptr;       // per sorted trace (BF16/F16), else nullptr
   float* accum = nullptr;        // adjoint accumulation rows (n_traces x row_stride f32)
+  // adjoint: tiles holding each block of adj_tb consecutive sorted traces, and
+  // the per-call column table (z'^2, a', g, threshold) per output sample
+  int adj_tb = 0;
+  int64_t* adj_off = nullptr;    // n_trace_blocks + 1
+  int* adj_tiles = nullptr;
+  int64_t n_adj_tiles = 0;
+  float4* adj_table = nullptr;   // n_times x n_il x n_xl, column-major
   int* err = nullptr;            // device error flags
   int64_t bytes = 0;
   bool traces_loaded = false;

@@ -162,12 +162,10 @@ bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out) {
 }
 
 size_t forward_smem_bytes(const Plan* p) {
-  // pipelined forward kernel: the smallest ring (2 stages x 1 row) must fit;
-  // the adjoint kernel needs 8 float accumulator rows
+  // pipelined forward kernel: the smallest ring (2 stages x 1 row) must fit
+  // (the adjoint keeps as many float rows as fit, at least one)
   const int T = p->shape.t_window();
-  const size_t fwd = (size_t)smem2_layout(p->shape.cols, T, p->row_stride, p->elt_bytes, 2, 1).total;
-  const size_t adj = (size_t)smem_layout(p->shape.cols, T, p->row_stride, 4, OP_ADJ).total;
-  return fwd > adj ? fwd : adj;
+  return (size_t)smem2_layout(p->shape.cols, T, p->row_stride, p->elt_bytes, 2, 1).total;
 }
 
 pstm_status launch_velocity_check(Plan* p, const float* vel, int64_t vst, int64_t vsc,

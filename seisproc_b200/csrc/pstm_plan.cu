@@ -526,6 +526,9 @@ static void free_plan(Plan* p) {
   cudaFree(p->perm);
   cudaFree(p->inv_perm);
   cudaFree(p->tile_off);
+  cudaFree(p->adj_off);
+  cudaFree(p->adj_tiles);
+  cudaFree(p->adj_table);
   cudaFree(p->tile_list);
   cudaFree(p->traces);
   cudaFree(p->scales);
@@ -912,8 +915,8 @@ pstm_status pstm_demigrate(pstm_plan* plan, const float* image, const float* vel
   const int64_t n = p->n_traces;
   const int n_s = p->n_samples;
   if (n == 0) return PSTM_OK;
+  // every sample of every row is written by the adjoint kernel: no clearing
   if (!p->accum) CUDA_TRY(dalloc(p, &p->accum, (size_t)n * p->row_stride));
-  CUDA_TRY(cudaMemsetAsync(p->accum, 0, (size_t)n * p->row_stride * sizeof(float), s));
   std::string why;
   st = launch_velocity_check(p, vel, vst, vsc, s, &why);
   if (st != PSTM_OK) return fail(st, why);
