@@ -22,14 +22,16 @@ import torch
 SHAPES: Dict[int, Tuple[int, int, int, int]] = {
     1: (8, 2, 4, 1024),
     2: (4, 2, 2, 1024),
+    3: (16, 4, 4, 512),
     4: (4, 2, 2, 512),
     5: (8, 8, 1, 1024),
     6: (4, 4, 1, 512),
     7: (2, 2, 1, 512),
     8: (4, 4, 1, 1024),
+    9: (16, 16, 1, 512),
 }
-LINE_SHAPES = (5, 6, 7, 8)
-GRID_SHAPES = (1, 2, 4)
+LINE_SHAPES = (5, 6, 7, 8, 9)
+GRID_SHAPES = (1, 2, 3, 4)
 
 _CACHE_PATH = os.environ.get("SEISPSTM_TUNE_CACHE",
                              os.path.join(os.path.expanduser("~"), ".cache", "seispstm_tune.json"))

@@ -299,6 +299,9 @@ cudaError_t adj_dispatch(const Plan* p, const KArgs& A, const float4* tab, cudaS
       return adj_wm<4, 2, 4>(p, A, tab, s);
     case 7:
       return adj_wm<2, 4, 2>(p, A, tab, s);
+    case 3:
+    case 9:
+      return adj_wm<16, 1, 8>(p, A, tab, s);
   }
   return cudaErrorInvalidValue;
 }

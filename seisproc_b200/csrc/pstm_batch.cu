@@ -109,6 +109,9 @@ cudaError_t batch_dispatch(const Batch* b, cudaStream_t s) {
       return batch_st<4, 2, 4>(b, s);
     case 7:
       return batch_st<2, 4, 2>(b, s);
+    case 3:
+    case 9:
+      return batch_st<16, 1, 8>(b, s);
   }
   return cudaErrorInvalidValue;
 }

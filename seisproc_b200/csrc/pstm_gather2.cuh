@@ -642,6 +642,9 @@ inline cudaError_t dispatch2_shape(const Plan* p, const KArgs& A, cudaStream_t s
       return dispatch2_st<4, 2, 4, OP>(p, A, s);
     case 7:
       return dispatch2_st<2, 4, 2, OP>(p, A, s);
+    case 3:
+    case 9:
+      return dispatch2_st<16, 1, 8, OP>(p, A, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -135,11 +135,13 @@ __global__ void pstm_velocity_check_kernel(const KArgs A, int n_cols_checked) {
 static const Shape kShapes[] = {
     {1, 8, 2, 8, 2, 4},  // 8 columns (2x4) x 1024 samples, 16 warps
     {2, 4, 4, 4, 2, 2},  // 4 columns (2x2) x 1024 samples, 16 warps
+    {3, 16, 1, 8, 4, 4},  // 16 columns (4x4) x 512 samples, 16 warps
     {4, 4, 2, 4, 2, 2},  // 4 columns (2x2) x 512 samples, 8 warps
     {5, 8, 2, 8, 8, 1},  // 2D lines: 8 inlines x 1024 samples
     {6, 4, 2, 4, 4, 1},  // 2D lines: 4 inlines x 512 samples
     {7, 2, 4, 2, 2, 1},  // 2D lines: 2 inlines x 512 samples
     {8, 4, 4, 4, 4, 1},  // 2D lines: 4 inlines x 1024 samples
+    {9, 16, 1, 8, 16, 1},  // 2D lines: 16 inlines x 512 samples
 };
 
 bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out) {
@@ -148,9 +150,9 @@ bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out) {
     // short output traces use 512-sample windows
     const bool line = n_xl < 2;
     if (line)
-      variant = n_times <= 512 ? 7 : 8;
+      variant = n_times <= 512 ? 9 : 8;
     else
-      variant = n_times <= 512 ? 4 : 1;
+      variant = n_times <= 512 ? 3 : 1;
   }
   for (const Shape& s : kShapes) {
     if (s.id == variant) {
