@@ -189,6 +189,7 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
     Plan* p = b->plans[i];
     descs[i] = make_args(p, velocity, v_stride_t, v_stride_c);
     descs[i].out = b->images[i];
+    descs[i].fold_out = b->folds[i];  // fold counted in the same launch (or nullptr)
     descs[i].ring_stages = b->ring_stages;
     descs[i].ring_rows = b->ring_rows;
     std::vector<int64_t> off(p->n_tiles + 1);
@@ -238,11 +239,6 @@ pstm_status pstm_batch_migrate(pstm_batch* batch, void* stream) {
   cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
   if (e == cudaSuccess && b->n_items > 0) e = batch_dispatch(b, s);
   if (e != cudaSuccess) return bfail(PSTM_ECUDA, std::string("batch kernel: ") + cudaGetErrorString(e));
-  for (size_t i = 0; i < b->plans.size(); ++i) {
-    if (!b->folds[i]) continue;
-    st = launch_fold(b->plans[i], b->vel, b->vst, b->vsc, b->folds[i], s, &why);
-    if (st != PSTM_OK) return bfail(st, why);
-  }
   return PSTM_OK;
 }
 

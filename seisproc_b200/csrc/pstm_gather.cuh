@@ -29,6 +29,7 @@ struct KArgs {
   int tda;
   float clamp_hi;
   float* out;
+  float* fold_out;  // forward: fold written alongside the image when non-null
   const float* in_img;
   float* accum;
   int* err;
@@ -138,6 +139,7 @@ inline KArgs make_args(const Plan* p, const float* vel, int64_t vst, int64_t vsc
   A.clamp_hi = p->params.clamp == PSTM_CLAMP_MIGRATOR ? (float)(p->n_samples - 2)
                                                       : (float)((double)p->n_samples - 1.001);
   A.out = nullptr;
+  A.fold_out = nullptr;
   A.in_img = nullptr;
   A.accum = p->accum;
   A.err = p->err;

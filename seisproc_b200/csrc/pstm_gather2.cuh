@@ -23,7 +23,7 @@ constexpr int kRowGuard = 16;
 constexpr int kSmemBudget = 227 * 1024;
 
 struct Smem2 {
-  int bars, thr, raw, total;
+  int bars, thr, hist, raw, total;
 };
 // Ring of `stages` stages of `sb` trace rows each.
 __host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, int stages, int sb) {
@@ -33,6 +33,8 @@ __host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, i
   o += 2 * kMaxStages * 8 + 16;
   o = (o + 15) & ~15;
   L.thr = o;
+  o += cols * T * 4;
+  L.hist = o;  // fold histogram of first contributing samples
   o += cols * T * 4;
   o = (o + 127) & ~127;
   L.raw = o;
@@ -274,6 +276,8 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   uint64_t* empty = full + kMaxStages;
   int* abort_flag = reinterpret_cast<int*>(empty + kMaxStages);
   float* thr = reinterpret_cast<float*>(smem + L.thr);
+  int* hist = reinterpret_cast<int*>(smem + L.hist);
+  const bool want_fold = A.fold_out != nullptr;
   unsigned char* raw = smem + L.raw;
   const int RP = S * ES + kRowGuard;  // bytes per staged row incl. its guard
 
@@ -306,6 +310,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     float v = -1.0f;
     if (kk < nk && tile_column(A, tile, q, qil, qxl)) v = threshold(A, qil * A.n_xl + qxl, k0 + kk);
     thr[e] = v;
+    if (want_fold) hist[e] = 0;
   }
   __syncthreads();
 
@@ -387,7 +392,11 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
       if (warp_live) {
         leg_h2(xc, yc, g_next, hs2, hr2);
         const int fv = first_valid(thr_c, nk, sqrtf(fmaxf(hs2, hr2)));
-        if (fv < nk) ks = k0 + fv;
+        if (fv < nk) {
+          ks = k0 + fv;
+          // fold: one warp per column counts where each trace starts
+          if (want_fold && ts == 0) atomicAdd(hist + cl * T + fv, 1);
+        }
         if constexpr (AA) {
           gxs = (xc - g_next.x) * A.aa_dx;
           gxr = (xc - g_next.z) * A.aa_dx;
@@ -503,9 +512,31 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     if (warp == 0 && lane == 0)
       for (int b = blk; b < min(nb, blk + kStages); ++b)
         mbar_wait(full + b % kStages, (b / kStages) & 1);
-    return;
   }
-  if (!warp_live) return;
+  if (want_fold) {
+    // fold = running count of the traces started so far (every warp of the
+    // CTA reaches this barrier, aborted or not)
+    __syncthreads();
+    if (warp < COLS && !*abort_flag) {
+      int qil, qxl;
+      if (tile_column(A, tile, warp, qil, qxl)) {
+        const int qc = qil * A.n_xl + qxl;
+        int carry = 0;
+        for (int base = 0; base < nk; base += 32) {
+          int v = (base + lane < nk) ? hist[warp * T + base + lane] : 0;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+          }
+          v += carry;
+          if (base + lane < nk) A.fold_out[(long long)(k0 + base + lane) * n_c + qc] = (float)v;
+          carry = __shfl_sync(0xffffffffu, v, 31);
+        }
+      }
+    }
+  }
+  if (aborted || !warp_live) return;
 #pragma unroll
   for (int i = 0; i < M; ++i) {
     const int klo = kw + 64 * i + lane, khi = klo + 32;

@@ -62,8 +62,9 @@ struct Plan {
 };
 
 // launchers (pstm_migrate.cu)
+// forward migration; fold (nullable) is counted in the same launch
 pstm_status launch_forward(Plan* p, const float* vel, int64_t vst, int64_t vsc, float* image,
-                           cudaStream_t s, std::string* why);
+                           float* fold, cudaStream_t s, std::string* why);
 pstm_status launch_fold(Plan* p, const float* vel, int64_t vst, int64_t vsc, float* fold,
                         cudaStream_t s, std::string* why);
 pstm_status launch_adjoint(Plan* p, const float* image, const float* vel, int64_t vst,

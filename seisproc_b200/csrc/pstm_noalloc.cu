@@ -305,7 +305,8 @@ extern "C" pstm_status pstm_migrate_noalloc(const pstm_grid* grid, const pstm_pa
   std::string why;
   if ((st = launch_velocity_check(&p, velocity, v_stride_t, v_stride_c, s, &why)) != PSTM_OK)
     return noalloc_fail(st, why);
-  if ((st = launch_forward(&p, velocity, v_stride_t, v_stride_c, image, s, &why)) != PSTM_OK)
+  if ((st = launch_forward(&p, velocity, v_stride_t, v_stride_c, image, nullptr, s, &why)) !=
+      PSTM_OK)
     return noalloc_fail(st, why);
   if (fold && (st = launch_fold(&p, velocity, v_stride_t, v_stride_c, fold, s, &why)) != PSTM_OK)
     return noalloc_fail(st, why);

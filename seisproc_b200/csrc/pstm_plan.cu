@@ -875,12 +875,8 @@ pstm_status pstm_migrate_loaded(pstm_plan* plan, const float* vel, int64_t vst, 
   std::string why;
   st = launch_velocity_check(p, vel, vst, vsc, s, &why);
   if (st != PSTM_OK) return fail(st, why);
-  st = launch_forward(p, vel, vst, vsc, image, s, &why);
+  st = launch_forward(p, vel, vst, vsc, image, fold, s, &why);
   if (st != PSTM_OK) return fail(st, why);
-  if (fold) {
-    st = launch_fold(p, vel, vst, vsc, fold, s, &why);
-    if (st != PSTM_OK) return fail(st, why);
-  }
   return PSTM_OK;
 }
 
