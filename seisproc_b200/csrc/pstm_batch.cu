@@ -60,7 +60,7 @@ template <int COLS, int WPC, int M, typename ST>
 cudaError_t batch_wm(const Batch* b, cudaStream_t s) {
   const Plan* p = b->plans[0];
   const bool lc = needs_lowclamp(p);
-  if constexpr (!std::is_same<ST, float>::value) {
+  if constexpr (!std::is_same<ST, float2>::value) {
     if (p->params.weight != W_OBL_SPREAD) return cudaErrorNotSupported;
     return lc ? launch_batch_one<COLS, WPC, M, ST, W_OBL_SPREAD, true>(b, s)
               : launch_batch_one<COLS, WPC, M, ST, W_OBL_SPREAD, false>(b, s);
@@ -87,7 +87,7 @@ template <int COLS, int WPC, int M>
 cudaError_t batch_st(const Batch* b, cudaStream_t s) {
   switch (b->plans[0]->params.storage) {
     case PSTM_F32:
-      return batch_wm<COLS, WPC, M, float>(b, s);
+      return batch_wm<COLS, WPC, M, float2>(b, s);
     case PSTM_BF16:
       return batch_wm<COLS, WPC, M, __nv_bfloat16>(b, s);
     case PSTM_F16:

@@ -150,6 +150,12 @@ struct Storage<float> {
   static constexpr int kAlign = 4;  // elements per 16 bytes
   __device__ __forceinline__ static float load(const float* p, int i) { return p[i]; }
 };
+// float32 samples expanded to (x[i], x[i+1] - x[i]) entries: one 8-byte load
+// gives both interpolation taps
+template <>
+struct Storage<float2> {
+  static constexpr int kAlign = 2;  // entries per 16 bytes
+};
 template <>
 struct Storage<__nv_bfloat16> {
   static constexpr int kAlign = 8;

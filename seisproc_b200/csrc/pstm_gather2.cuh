@@ -1,15 +1,16 @@
 // Warp-specialised gather kernel (forward migration and V-gradient).
 //
 // The rows of the tile's trace list stream through a ring of up to 4
-// shared-memory stages (up to 8 rows each) by 1-D TMA bulk copies issued by
-// lane 0 of warp 0; `full[s]` completes on the copies' byte count, `empty[s]`
+// shared-memory stages (up to 32 rows each) by 1-D TMA bulk copies issued by
+// warp 0 (one row per lane); `full[s]` completes on the copies' byte count, `empty[s]`
 // when every warp has finished the stage.  Warps never synchronise with each
 // other otherwise (warp 0 waits on `empty` before refilling): each one computes
 // the per-(column, trace) set-up for 32 list entries at a time (one lane per
 // trace: leg distances and the first contributing sample by binary search in
 // the CTA's threshold table), then sweeps the traces, taking each trace's
 // set-up from its lane by shuffle.  Samples are read straight from the staged
-// row: two shared loads (x[i0], x[i0+1]) and one f32x2 FMA per sample pair.
+// row: float32 rows hold expanded (x[i], x[i+1] - x[i]) entries (one 8-byte
+// load and one FMA per sample), 16-bit rows plain samples (two loads).
 #pragma once
 #include "pstm_gather.cuh"
 
@@ -43,7 +44,9 @@ __host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, i
   return L;
 }
 
-// Largest ring (up to 4 stages x 8 rows, at least 2 stages) that fits.
+// Ring of the largest stages (up to 32 rows), then the most stages (up to 4,
+// at least 2), that fits: large stages measured faster than deeper rings of
+// smaller ones (fewer barrier round trips per trace).
 inline bool ring_shape(int cols, int T, int S, int elt, int* stages, int* sb) {
   for (int b = kBlockTraces; b >= 1; b >>= 1)
     for (int st = kMaxStages; st >= 2; --st)
@@ -102,7 +105,7 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
                                              const float (&sc)[NTR], f2 bb, float hi_c,
                                              float lo_c, int kw, int lane, int g0) {
   constexpr int ES = (int)sizeof(ST);
-  constexpr int SHIFT = ES == 4 ? 2 : 1;
+  constexpr int SHIFT = ES == 8 ? 3 : (ES == 4 ? 2 : 1);
   const f2 magic2 = f2_bcast(kMagic);
 #pragma unroll
   for (int i = 0; i < M; ++i) {
@@ -140,10 +143,18 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
       const f2 fr = f2_sub(id, f2_sub(tm, magic2));
       const uint32_t a0 = rbase[n] + (__float_as_uint(tm.x) << SHIFT);
       const uint32_t a1 = rbase[n] + (__float_as_uint(tm.y) << SHIFT);
-      const f2 x0 = f2{lds_elem<ST>(a0), lds_elem<ST>(a1)};
-      const f2 x1 = f2{lds_elem<ST>(a0 + ES), lds_elem<ST>(a1 + ES)};
-      const f2 dx = f2_sub(x1, x0);
-      const f2 amp = f2_fma(fr, dx, x0);
+      f2 dx, amp;
+      if constexpr (std::is_same<ST, float2>::value) {
+        // expanded rows: one 8-byte load gives (x[i0], x[i0+1] - x[i0])
+        const f2 e0 = lds_f2(a0), e1 = lds_f2(a1);
+        dx = f2{e0.y, e1.y};
+        amp = f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
+      } else {
+        const f2 x0 = f2{lds_elem<ST>(a0), lds_elem<ST>(a1)};
+        const f2 x1 = f2{lds_elem<ST>(a0 + ES), lds_elem<ST>(a1 + ES)};
+        dx = f2_sub(x1, x0);
+        amp = f2_fma(fr, dx, x0);
+      }
       const f2 p = f2_mul(qs, qr);
       if constexpr (kPrescaled<OP, WM>) {
         // weight p^2 (obliquity x spreading; the a^4 z^2 factor comes in the
@@ -214,11 +225,10 @@ __device__ __forceinline__ void sweep_aa(f2 (&acc)[M], const f2 (&zz)[M], const 
   auto tap = [&](f2 pos, uint32_t base) {
     const f2 tm = f2_add_rm(pos, magic2);
     const f2 fr = f2_sub(pos, f2_sub(tm, magic2));
-    const uint32_t a0 = base + (__float_as_uint(tm.x) << 2);
-    const uint32_t a1 = base + (__float_as_uint(tm.y) << 2);
-    const f2 x0 = f2{lds_elem<float>(a0), lds_elem<float>(a1)};
-    const f2 x1 = f2{lds_elem<float>(a0 + 4), lds_elem<float>(a1 + 4)};
-    return f2_fma(fr, f2_sub(x1, x0), x0);
+    // expanded rows: (I2[e], I2[e+1] - I2[e]) per 8-byte entry
+    const f2 e0 = lds_f2(base + (__float_as_uint(tm.x) << 3));
+    const f2 e1 = lds_f2(base + (__float_as_uint(tm.y) << 3));
+    return f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
   };
 #pragma unroll
   for (int i = 0; i < M; ++i) {
@@ -267,7 +277,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   constexpr int NW = COLS * WPC;
   constexpr int T = WPC * 64 * M;
   constexpr int ES = (int)sizeof(ST);
-  constexpr int SHIFT = ES == 4 ? 2 : 1;
+  constexpr int SHIFT = ES == 8 ? 3 : (ES == 4 ? 2 : 1);
   static_assert(kRowGuard % 16 == 0, "row data must stay 16-byte aligned");
   const int S = A.S;
   const int B = A.ring_rows, kStages = A.ring_stages;
@@ -364,7 +374,9 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     acc[i] = f2{0.f, 0.f};
   }
   // staged position of sample index idx: idx - lo (plain) or idx + pad (AA)
-  const float shift = AA ? (float)A.aa_pad : -(float)lo;
+  // (expanded float32 rows hold sample i at entry i + 1)
+  constexpr bool kExpanded = std::is_same<ST, float2>::value;
+  const float shift = AA ? (float)A.aa_pad : (kExpanded ? 1.0f : 0.0f) - (float)lo;
   const float bconst = -A.in_t0 / A.in_dt + shift;
   const f2 bb = f2_bcast(bconst);
   const float hi_c = A.clamp_hi + shift;
@@ -622,7 +634,8 @@ inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
 template <int COLS, int WPC, int M, typename ST, int OP>
 inline cudaError_t dispatch2_wm(const Plan* p, const KArgs& A, cudaStream_t s) {
   const int wm = p->params.weight;
-  if constexpr (OP == OP_VGRAD || !std::is_same<ST, float>::value) {
+  constexpr bool k32 = std::is_same<ST, float>::value || std::is_same<ST, float2>::value;
+  if constexpr (OP == OP_VGRAD || !k32) {
     if (wm != W_OBL_SPREAD) return cudaErrorNotSupported;
     return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP>(p, A, s);
   } else {
@@ -644,13 +657,15 @@ template <int COLS, int WPC, int M, int OP>
 inline cudaError_t dispatch2_st(const Plan* p, const KArgs& A, cudaStream_t s) {
   if (p->params.antialias) {
     if constexpr (OP == OP_FWD)
-      return launch2_one<COLS, WPC, M, float, W_OBL_SPREAD, OP, true>(p, A, s);
+      return launch2_one<COLS, WPC, M, float2, W_OBL_SPREAD, OP, true>(p, A, s);
     else
       return cudaErrorNotSupported;
   }
   switch (p->params.storage) {
     case PSTM_F32:
-      return dispatch2_wm<COLS, WPC, M, float, OP>(p, A, s);
+      // plans stage expanded (x, dx) rows; the no-allocation path plain rows
+      return p->elt_bytes == 8 ? dispatch2_wm<COLS, WPC, M, float2, OP>(p, A, s)
+                               : dispatch2_wm<COLS, WPC, M, float, OP>(p, A, s);
     case PSTM_BF16:
       return dispatch2_wm<COLS, WPC, M, __nv_bfloat16, OP>(p, A, s);
     case PSTM_F16:

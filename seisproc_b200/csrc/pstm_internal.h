@@ -21,7 +21,7 @@ struct Shape {
 };
 
 constexpr int kGuard = 2;        // guard entries before the first staged sample
-constexpr int kBlockTraces = 8;  // traces staged per pipeline step
+constexpr int kBlockTraces = 32;  // trace rows per pipeline stage, at most
 
 struct Plan {
   int device = 0;

@@ -326,6 +326,42 @@ __global__ void stage_rows_kernel(const float* tr, int64_t n_tr, int n_s, const 
     out[jj * S + i] = convert_to<ST>(tr[(int64_t)j * n_s + i] * inv);
 }
 
+// float32 staging into (x[i], x[i+1] - x[i]) entries at row position i + 1
+// (x = 0 outside the trace), sample-major input via 33 x 32 shared tiles.
+__global__ void stage_transpose_x2_kernel(const float* tr, int64_t n_tr, int n_s,
+                                          const int* inv_perm, int S, float2* out) {
+  __shared__ float tile[33][33];
+  const int64_t j0 = (int64_t)blockIdx.x * 32;
+  const int i0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 33; r += blockDim.y) {
+    const int i = i0 + r;
+    const int64_t j = j0 + threadIdx.x;
+    tile[r][threadIdx.x] = (i < n_s && j < n_tr) ? tr[(int64_t)i * n_tr + j] : 0.f;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t j = j0 + r;
+    const int i = i0 + threadIdx.x;
+    if (j < n_tr && i < n_s) {
+      const int jj = inv_perm[j];
+      const float x0 = tile[threadIdx.x][r], x1 = tile[threadIdx.x + 1][r];
+      out[(int64_t)jj * S + i + 1] = make_float2(x0, x1 - x0);
+      if (i == 0) out[(int64_t)jj * S] = make_float2(0.f, x0);
+    }
+  }
+}
+
+__global__ void stage_rows_x2_kernel(const float* tr, int64_t n_tr, int n_s, const int* perm,
+                                     int S, float2* out) {
+  const int64_t jj = blockIdx.x;
+  const float* x = tr + (int64_t)perm[jj] * n_s;
+  for (int i = (int)threadIdx.x - 1; i < n_s; i += blockDim.x) {
+    const float x0 = i >= 0 ? x[i] : 0.f;
+    const float x1 = i + 1 < n_s ? x[i + 1] : 0.f;
+    out[jj * S + i + 1] = make_float2(x0, x1 - x0);
+  }
+}
+
 // sorted trace-major accumulation rows -> caller layout, original order
 __global__ void unstage_transpose_kernel(const float* acc, int64_t n_tr, int n_s,
                                          const int* inv_perm, int S, float* out) {
@@ -367,12 +403,17 @@ __device__ __forceinline__ float quantize_sample(float x, int storage, float sca
 }
 
 __global__ void aa_integrate_kernel(const float* rows, int64_t n_tr, int n_s, int S_in, int storage,
-                                    int pad, int S_out, float* out) {
+                                    int pad, int S_out, float2* out) {
   const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= n_tr) return;
   const float* x = rows + row * S_in;
-  float* o = out + row * S_out;
+  float2* o = out + row * S_out;
+  // entry at position i + pad: (I2'[i], I2'[i+1] - I2'[i]) of the float32 values
+  auto entry = [](double cur, double nxt) {
+    const float c = (float)cur;
+    return make_float2(c, (float)nxt - c);
+  };
   float scale = 1.0f;
   if (storage == PSTM_F16) {
     float m = 0.f;
@@ -416,7 +457,9 @@ __global__ void aa_integrate_kernel(const float* rows, int64_t n_tr, int n_s, in
       const double u = __shfl_up_sync(0xffffffffu, acc, d);
       if (lane >= d) acc += u;
     }
-    if (i < n_s) o[i + pad] = (float)(c2 + acc - beta * (double)i);
+    // I2[i+1] = I2[i] + I1[i]
+    if (i < n_s) o[i + pad] = entry(c2 + acc - beta * (double)i,
+                                    c2 + acc + i1 - beta * (double)(i + 1));
     double e = i < n_s ? i1 : 0.0;
     for (int d = 16; d > 0; d >>= 1) e += __shfl_xor_sync(0xffffffffu, e, d);
     c1 = __shfl_sync(0xffffffffu, i1, 31);
@@ -425,11 +468,12 @@ __global__ void aa_integrate_kernel(const float* rows, int64_t n_tr, int n_s, in
   // before the trace (I2 = 0) and from I2[N] on (linear continuation)
   for (int q = lane; q < pad; q += 32) {
     const int i = q - pad;  // -pad .. -1
-    o[q] = (float)(-beta * (double)i);
+    o[q] = entry(-beta * (double)i, -beta * (double)(i + 1));
   }
   for (int q = n_s + pad + lane; q < S_out; q += 32) {
-    const int i = q - pad;  // N .. 
-    o[q] = (float)(i2_end + (double)(i - n_s) * i1_last - beta * (double)i);
+    const int i = q - pad;  // N ..
+    o[q] = entry(i2_end + (double)(i - n_s) * i1_last - beta * (double)i,
+                 i2_end + (double)(i + 1 - n_s) * i1_last - beta * (double)(i + 1));
   }
 }
 
@@ -619,12 +663,17 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
   p->n_traces = geo->n_traces;
   p->n_samples = prm->n_samples;
   p->row_stride = (int)align_up(prm->n_samples, 8);
-  p->elt_bytes = prm->storage == PSTM_F32 ? 4 : 2;
+  p->elt_bytes = 2;
+  if (prm->storage == PSTM_F32) {
+    // (x[i], x[i+1] - x[i]) entries for i = -1 .. N-1 at row positions i + 1
+    p->row_stride = (int)align_up(prm->n_samples + 1, 8);
+    p->elt_bytes = 8;
+  }
   if (prm->antialias) {
     // rows hold the trend-removed double integral I2[-pad .. N + pad] in float32
     p->aa_pad = (int)std::ceil(prm->aa_max_halfwidth) + 2;
     p->row_stride = (int)align_up(prm->n_samples + 1 + 2 * p->aa_pad, 8);
-    p->elt_bytes = 4;
+    p->elt_bytes = 8;  // (I2[i], I2[i+1] - I2[i]) entries
   }
   if (!shape_for_variant(prm->variant, g->n_xl, g->n_times, &p->shape))
     return fail(PSTM_EINVAL, "unknown kernel variant");
@@ -825,7 +874,7 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
     LAUNCH_CHECK("stage kernel");
     aa_integrate_kernel<<<(unsigned)((n + 7) / 8), 256, 0, s>>>(
         p->accum, n, n_s, S_in, p->params.storage, p->aa_pad, p->row_stride,
-        reinterpret_cast<float*>(p->traces));
+        reinterpret_cast<float2*>(p->traces));
     LAUNCH_CHECK("aa_integrate_kernel");
     p->traces_loaded = true;
     return PSTM_OK;
@@ -846,7 +895,12 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
     stage_transpose_kernel<T><<<tg, tb, 0, s>>>(traces, n, n_s, p->inv_perm, p->scales,       \
                                                 p->row_stride, (T*)p->traces);
   if (p->params.storage == PSTM_F32) {
-    PSTM_STAGE(float)
+    if (trace_major)
+      stage_rows_x2_kernel<<<(unsigned)n, 256, 0, s>>>(traces, n, n_s, p->perm, p->row_stride,
+                                                       (float2*)p->traces);
+    else
+      stage_transpose_x2_kernel<<<tg, tb, 0, s>>>(traces, n, n_s, p->inv_perm, p->row_stride,
+                                                  (float2*)p->traces);
   } else if (p->params.storage == PSTM_BF16) {
     PSTM_STAGE(__nv_bfloat16)
   } else {
