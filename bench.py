@@ -43,9 +43,9 @@ sys.path.insert(0, ROOT)
 MUFU_PER_SM_CLK = 16
 RSQRT_PER_PAIR = 2
 # DRAM bytes per trace-list entry of the forward gather, from the ncu capture
-# of the 100k-trace case (7.56 GB / 17.35 M entries; profiles/pstm_gather_forward_3d.md);
+# of the 100k-trace case (51.6 GB / 17.35 M entries, expanded float32 rows);
 # the traffic of a full launch is scaled by its list entries.
-DRAM_BYTES_PER_LIST_ENTRY = 436.0
+DRAM_BYTES_PER_LIST_ENTRY = 2972.0
 
 
 def peaks():
@@ -514,7 +514,7 @@ def bench_lsq(args):
     from seisproc_b200.kirchhoff import PSTMPlan
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
-    s = synthetic.survey_3d(n_traces=120_000, seed=7, device=dev, n_samples=500, dt_ms=2.0,
+    s = synthetic.survey_3d(n_traces=args.lsq_traces, seed=7, device=dev, n_samples=500, dt_ms=2.0,
                             extent=2500.0, max_offset=1500.0, n_il=100, n_xl=100, spacing=25.0,
                             n_diffractors=60, aperture=1000.0)
     c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -536,7 +536,7 @@ def bench_lsq(args):
     tt = np.linspace(0.0, 1.0, s.n_times)[:, None, None]
     xx = np.linspace(0.0, 1.0, s.n_il)[None, :, None]
     yy = np.linspace(0.0, 1.0, s.n_xl)[None, None, :]
-    for _ in range(20):
+    for _ in range(args.fd_directions):
         # smooth random perturbation (keeps V t0 increasing in t0)
         c = rs.randn(4)
         f = (c[0] + c[1] * np.sin(np.pi * (tt + rs.rand())) + c[2] * np.cos(2 * np.pi * xx)
@@ -548,16 +548,18 @@ def bench_lsq(args):
     fd, an = np.array(fd), np.array(an)
     plan.check()
     d = plan.demigrate(migrate(tr, v, plan), v)  # data in the range of L
-    m, hist = cgls(plan, d, v, n_iter=10)
+    m, hist = cgls(plan, d, v, n_iter=args.cg_iters)
     it_s = [h[2] for h in hist[1:]]
     print(json.dumps({
         "metric": "LSQ PSTM CG seconds per iteration", "value": float(np.median(it_s)),
         "unit": "s/iter", "n_gpus": 1, "higher_is_better": False, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": "least-squares PSTM 100x100x500, 120k traces at 2 ms, FP32"},
+        "config": {"workload": f"least-squares PSTM 100x100x500, {args.lsq_traces // 1000}k "
+                               "traces at 2 ms, FP32", "cg_iterations": args.cg_iters},
         "dot_product": {"<Lm,d>": a_, "<m,L^T d>": b_, "rel": rel},
-        "vgrad_fd": {"rel_l2_over_20_directions": float(np.linalg.norm(fd - an) /
-                                                         np.linalg.norm(fd)),
+        "vgrad_fd": {"directions": args.fd_directions,
+                     "rel_l2": float(np.linalg.norm(fd - an) / np.linalg.norm(fd))
+                     if args.fd_directions else None,
                      "note": "noisy 30 Hz data from t0 = 0: includes interpolation kinks and "
                              "mask switches"},
         "cg": {"residual_history": [h[1] for h in hist], "misfit_reduction": hist[-1][1]},
@@ -586,6 +588,9 @@ def main():
     ap.add_argument("--aa-lmax", type=float, default=32.0)
     ap.add_argument("--utm", action="store_true",
                     help="world coordinates offset by a UTM origin (5e5, 6e6) m")
+    ap.add_argument("--lsq-traces", type=int, default=120_000)
+    ap.add_argument("--cg-iters", type=int, default=10)
+    ap.add_argument("--fd-directions", type=int, default=20)
     ap.add_argument("--config", default="3d", choices=["3d", "batched", "lsq"])
     args = ap.parse_args()
     if args.config == "batched" and args.impl == "ours":
