@@ -43,9 +43,9 @@ sys.path.insert(0, ROOT)
 MUFU_PER_SM_CLK = 16
 RSQRT_PER_PAIR = 2
 # DRAM bytes per trace-list entry of the forward gather, from the ncu capture
-# of the 100k-trace case (51.6 GB / 17.35 M entries, expanded float32 rows);
+# of the 100k-trace case (31.2 GB / 9.0 M entries, 16-column tiles, expanded float32 rows);
 # the traffic of a full launch is scaled by its list entries.
-DRAM_BYTES_PER_LIST_ENTRY = 2972.0
+DRAM_BYTES_PER_LIST_ENTRY = 3473.0
 
 
 def peaks():

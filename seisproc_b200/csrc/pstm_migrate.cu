@@ -146,13 +146,12 @@ static const Shape kShapes[] = {
 
 bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out) {
   if (variant == 0) {
-    // heuristic: square-ish tiles for 3D grids, inline strips for 2D lines;
-    // short output traces use 512-sample windows
+    // heuristic: 4 x 4 tiles for 3D grids, inline strips for 2D lines
     const bool line = n_xl < 2;
     if (line)
       variant = n_times <= 512 ? 9 : 8;
     else
-      variant = n_times <= 512 ? 3 : 1;
+      variant = 3;  // 16 columns x 512 samples: fastest measured for 500 and 1000 samples
   }
   for (const Shape& s : kShapes) {
     if (s.id == variant) {
