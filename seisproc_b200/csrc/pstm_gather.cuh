@@ -37,6 +37,7 @@ struct KArgs {
   // anti-alias: output spacing (m) per axis, max half-width (samples), row pad
   float aa_dx, aa_dy, aa_lmax;
   int aa_pad;
+  int row_origin;  // expanded rows: intercept origin (entry index)
 };
 
 __device__ __forceinline__ float vel_at(const KArgs& A, int k, int c) {
@@ -148,6 +149,7 @@ inline KArgs make_args(const Plan* p, const float* vel, int64_t vst, int64_t vsc
   A.aa_dy = (float)p->params.aa_dy;
   A.aa_lmax = (float)p->params.aa_max_halfwidth;
   A.aa_pad = p->aa_pad;
+  A.row_origin = p->row_origin;
   return A;
 }
 

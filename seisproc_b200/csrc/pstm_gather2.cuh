@@ -102,11 +102,10 @@ template <int M, typename ST, int WM, bool LOWC, bool MASKED, int OP, int NTR>
 __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], const f2 (&aa)[M],
                                              const float (&hs2)[NTR], const float (&hr2)[NTR],
                                              const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
-                                             const float (&sc)[NTR], f2 bb, float hi_c,
-                                             float lo_c, int kw, int lane, int g0) {
+                                             const float (&sc)[NTR], f2 bb, f2 magic2,
+                                             float hi_c, float lo_c, int kw, int lane, int g0) {
   constexpr int ES = (int)sizeof(ST);
   constexpr int SHIFT = ES == 8 ? 3 : (ES == 4 ? 2 : 1);
-  const f2 magic2 = f2_bcast(kMagic);
 #pragma unroll
   for (int i = 0; i < M; ++i) {
     if constexpr (MASKED) {
@@ -140,16 +139,17 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
         id.y = fmaxf(id.y, lo_c);
       }
       const f2 tm = f2_add_rm(id, magic2);
-      const f2 fr = f2_sub(id, f2_sub(tm, magic2));
       const uint32_t a0 = rbase[n] + (__float_as_uint(tm.x) << SHIFT);
       const uint32_t a1 = rbase[n] + (__float_as_uint(tm.y) << SHIFT);
       f2 dx, amp;
       if constexpr (std::is_same<ST, float2>::value) {
-        // expanded rows: one 8-byte load gives (x[i0], x[i0+1] - x[i0])
+        // expanded rows: one 8-byte load gives the piece's intercept and slope
+        // in the index frame, so the interpolant is one FMA of the index
         const f2 e0 = lds_f2(a0), e1 = lds_f2(a1);
         dx = f2{e0.y, e1.y};
-        amp = f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
+        amp = f2{fmaf(id.x, e0.y, e0.x), fmaf(id.y, e1.y, e1.x)};
       } else {
+        const f2 fr = f2_sub(id, f2_sub(tm, magic2));
         const f2 x0 = f2{lds_elem<ST>(a0), lds_elem<ST>(a1)};
         const f2 x1 = f2{lds_elem<ST>(a0 + ES), lds_elem<ST>(a1 + ES)};
         dx = f2_sub(x1, x0);
@@ -219,16 +219,14 @@ __device__ __forceinline__ void sweep_aa(f2 (&acc)[M], const f2 (&zz)[M], const 
                                          const float (&gxs)[NTR], const float (&gxr)[NTR],
                                          const float (&gys)[NTR], const float (&gyr)[NTR],
                                          const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
-                                         f2 bb, float hi_c, float lo_c, float lmax, int kw,
-                                         int lane, int g0) {
-  const f2 magic2 = f2_bcast(kMagic);
+                                         f2 bb, f2 magic2, float hi_c, float lo_c, float lmax,
+                                         int kw, int lane, int g0) {
   auto tap = [&](f2 pos, uint32_t base) {
+    // expanded rows: intercept and slope of I2's piece, one FMA of the position
     const f2 tm = f2_add_rm(pos, magic2);
-    const f2 fr = f2_sub(pos, f2_sub(tm, magic2));
-    // expanded rows: (I2[e], I2[e+1] - I2[e]) per 8-byte entry
     const f2 e0 = lds_f2(base + (__float_as_uint(tm.x) << 3));
     const f2 e1 = lds_f2(base + (__float_as_uint(tm.y) << 3));
-    return f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
+    return f2{fmaf(pos.x, e0.y, e0.x), fmaf(pos.y, e1.y, e1.x)};
   };
 #pragma unroll
   for (int i = 0; i < M; ++i) {
@@ -373,10 +371,15 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     }
     acc[i] = f2{0.f, 0.f};
   }
-  // staged position of sample index idx: idx - lo (plain) or idx + pad (AA)
-  // (expanded float32 rows hold sample i at entry i + 1)
+  // Index frame of the sweeps.  16-bit rows: the staged position idx - lo.
+  // Expanded rows (sample i at entry i + 1, or i + pad for the anti-alias
+  // integral): the entry coordinate less the rows' intercept origin q0; the
+  // rounding-down add of 2^23 + q0 - lo then yields the staged entry's index
+  // in the float's low bits.
   constexpr bool kExpanded = std::is_same<ST, float2>::value;
-  const float shift = AA ? (float)A.aa_pad : (kExpanded ? 1.0f : 0.0f) - (float)lo;
+  const float shift = kExpanded ? (AA ? (float)A.aa_pad : 1.0f) - (float)A.row_origin
+                                : -(float)lo;
+  const f2 mg = f2_bcast(kExpanded ? kMagic + (float)(A.row_origin - lo) : kMagic);
   const float bconst = -A.in_t0 / A.in_dt + shift;
   const f2 bb = f2_bcast(bconst);
   const float hi_c = A.clamp_hi + shift;
@@ -458,10 +461,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
           const uint32_t rb[1] = {rb0 + (uint32_t)(q * RP)};
           const int kk[1] = {kq};
           if (kq > kw)
-            sweep_aa<M, LOWC, true, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, hi_c,
+            sweep_aa<M, LOWC, true, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, mg, hi_c,
                                        lo_c, A.aa_lmax, kw, lane, (kq - kw) >> 6);
           else
-            sweep_aa<M, LOWC, false, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, hi_c,
+            sweep_aa<M, LOWC, false, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, mg, hi_c,
                                         lo_c, A.aa_lmax, kw, lane, 0);
         }
       } else if (la && lb) {
@@ -471,10 +474,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const uint32_t rb[2] = {rb0, rb0 + (uint32_t)RP};
         const int kk[2] = {ka, kb};
         if (ka > kw || kb > kw)
-          sweep_traces<M, ST, WM, LOWC, true, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
+          sweep_traces<M, ST, WM, LOWC, true, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c,
                                                       lo_c, kw, lane, (min(ka, kb) - kw) >> 6);
         else
-          sweep_traces<M, ST, WM, LOWC, false, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
+          sweep_traces<M, ST, WM, LOWC, false, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c,
                                                        lo_c, kw, lane, 0);
       } else if (la || lb) {
         const int u = la ? t : t + 1;
@@ -484,10 +487,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const uint32_t rb[1] = {la ? rb0 : rb0 + (uint32_t)RP};
         const int kk[1] = {la ? ka : kb};
         if (kk[0] > kw)
-          sweep_traces<M, ST, WM, LOWC, true, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
+          sweep_traces<M, ST, WM, LOWC, true, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c,
                                                       lo_c, kw, lane, (kk[0] - kw) >> 6);
         else
-          sweep_traces<M, ST, WM, LOWC, false, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, hi_c,
+          sweep_traces<M, ST, WM, LOWC, false, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c,
                                                        lo_c, kw, lane, 0);
       }
       const int adv = pair ? 2 : 1;

@@ -31,6 +31,7 @@ struct Plan {
   int n_samples = 0;
   int row_stride = 0;  // elements per staged trace row (multiple of 8)
   int aa_pad = 0;      // anti-alias rows: integral entries before sample 0 (and after N)
+  int row_origin = 0;  // expanded rows: entry q holds (x - (q - row_origin) dx, dx)
   int elt_bytes = 4;
   Shape shape{};
   int tiles_il = 0, tiles_xl = 0;

@@ -326,10 +326,20 @@ __global__ void stage_rows_kernel(const float* tr, int64_t n_tr, int n_s, const 
     out[jj * S + i] = convert_to<ST>(tr[(int64_t)j * n_s + i] * inv);
 }
 
-// float32 staging into (x[i], x[i+1] - x[i]) entries at row position i + 1
-// (x = 0 outside the trace), sample-major input via 33 x 32 shared tiles.
+// Expanded entry at row position q for the linear piece from x0 to x1:
+// (x0 - (q - q0) d, d) with d = x1 - x0 (float32), so that the interpolant at
+// position u in [q, q + 1) is one FMA, (u - q0) d + c, with no fractional part
+// to form.  The intercept is rounded once from float64; q0 (mid-row) keeps
+// |q - q0| small.
+__device__ __forceinline__ float2 expanded_entry(float x0, float x1, int q, int q0) {
+  const float d = x1 - x0;
+  return make_float2((float)((double)x0 - (double)(q - q0) * (double)d), d);
+}
+
+// float32 staging into expanded entries at row position i + 1 (x = 0 outside
+// the trace), sample-major input via 33 x 32 shared tiles.
 __global__ void stage_transpose_x2_kernel(const float* tr, int64_t n_tr, int n_s,
-                                          const int* inv_perm, int S, float2* out) {
+                                          const int* inv_perm, int S, int q0, float2* out) {
   __shared__ float tile[33][33];
   const int64_t j0 = (int64_t)blockIdx.x * 32;
   const int i0 = blockIdx.y * 32;
@@ -345,20 +355,20 @@ __global__ void stage_transpose_x2_kernel(const float* tr, int64_t n_tr, int n_s
     if (j < n_tr && i < n_s) {
       const int jj = inv_perm[j];
       const float x0 = tile[threadIdx.x][r], x1 = tile[threadIdx.x + 1][r];
-      out[(int64_t)jj * S + i + 1] = make_float2(x0, x1 - x0);
-      if (i == 0) out[(int64_t)jj * S] = make_float2(0.f, x0);
+      out[(int64_t)jj * S + i + 1] = expanded_entry(x0, x1, i + 1, q0);
+      if (i == 0) out[(int64_t)jj * S] = expanded_entry(0.f, x0, 0, q0);
     }
   }
 }
 
 __global__ void stage_rows_x2_kernel(const float* tr, int64_t n_tr, int n_s, const int* perm,
-                                     int S, float2* out) {
+                                     int S, int q0, float2* out) {
   const int64_t jj = blockIdx.x;
   const float* x = tr + (int64_t)perm[jj] * n_s;
   for (int i = (int)threadIdx.x - 1; i < n_s; i += blockDim.x) {
     const float x0 = i >= 0 ? x[i] : 0.f;
     const float x1 = i + 1 < n_s ? x[i + 1] : 0.f;
-    out[jj * S + i + 1] = make_float2(x0, x1 - x0);
+    out[jj * S + i + 1] = expanded_entry(x0, x1, i + 1, q0);
   }
 }
 
@@ -403,16 +413,15 @@ __device__ __forceinline__ float quantize_sample(float x, int storage, float sca
 }
 
 __global__ void aa_integrate_kernel(const float* rows, int64_t n_tr, int n_s, int S_in, int storage,
-                                    int pad, int S_out, float2* out) {
+                                    int pad, int S_out, int q0, float2* out) {
   const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= n_tr) return;
   const float* x = rows + row * S_in;
   float2* o = out + row * S_out;
-  // entry at position i + pad: (I2'[i], I2'[i+1] - I2'[i]) of the float32 values
-  auto entry = [](double cur, double nxt) {
-    const float c = (float)cur;
-    return make_float2(c, (float)nxt - c);
+  // expanded entry at position i + pad from the float32 values I2'[i], I2'[i+1]
+  auto entry = [&](double cur, double nxt, int i) {
+    return expanded_entry((float)cur, (float)nxt, i + pad, q0);
   };
   float scale = 1.0f;
   if (storage == PSTM_F16) {
@@ -459,7 +468,7 @@ __global__ void aa_integrate_kernel(const float* rows, int64_t n_tr, int n_s, in
     }
     // I2[i+1] = I2[i] + I1[i]
     if (i < n_s) o[i + pad] = entry(c2 + acc - beta * (double)i,
-                                    c2 + acc + i1 - beta * (double)(i + 1));
+                                    c2 + acc + i1 - beta * (double)(i + 1), i);
     double e = i < n_s ? i1 : 0.0;
     for (int d = 16; d > 0; d >>= 1) e += __shfl_xor_sync(0xffffffffu, e, d);
     c1 = __shfl_sync(0xffffffffu, i1, 31);
@@ -468,12 +477,12 @@ __global__ void aa_integrate_kernel(const float* rows, int64_t n_tr, int n_s, in
   // before the trace (I2 = 0) and from I2[N] on (linear continuation)
   for (int q = lane; q < pad; q += 32) {
     const int i = q - pad;  // -pad .. -1
-    o[q] = entry(-beta * (double)i, -beta * (double)(i + 1));
+    o[q] = entry(-beta * (double)i, -beta * (double)(i + 1), i);
   }
   for (int q = n_s + pad + lane; q < S_out; q += 32) {
     const int i = q - pad;  // N ..
     o[q] = entry(i2_end + (double)(i - n_s) * i1_last - beta * (double)i,
-                 i2_end + (double)(i + 1 - n_s) * i1_last - beta * (double)(i + 1));
+                 i2_end + (double)(i + 1 - n_s) * i1_last - beta * (double)(i + 1), i);
   }
 }
 
@@ -668,12 +677,14 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
     // (x[i], x[i+1] - x[i]) entries for i = -1 .. N-1 at row positions i + 1
     p->row_stride = (int)align_up(prm->n_samples + 1, 8);
     p->elt_bytes = 8;
+    p->row_origin = (prm->n_samples + 1) / 2;
   }
   if (prm->antialias) {
     // rows hold the trend-removed double integral I2[-pad .. N + pad] in float32
     p->aa_pad = (int)std::ceil(prm->aa_max_halfwidth) + 2;
     p->row_stride = (int)align_up(prm->n_samples + 1 + 2 * p->aa_pad, 8);
-    p->elt_bytes = 8;  // (I2[i], I2[i+1] - I2[i]) entries
+    p->elt_bytes = 8;  // intercept-form entries of I2
+    p->row_origin = (prm->n_samples + 1 + 2 * p->aa_pad) / 2;
   }
   if (!shape_for_variant(prm->variant, g->n_xl, g->n_times, &p->shape))
     return fail(PSTM_EINVAL, "unknown kernel variant");
@@ -873,7 +884,7 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
                                                       p->accum);
     LAUNCH_CHECK("stage kernel");
     aa_integrate_kernel<<<(unsigned)((n + 7) / 8), 256, 0, s>>>(
-        p->accum, n, n_s, S_in, p->params.storage, p->aa_pad, p->row_stride,
+        p->accum, n, n_s, S_in, p->params.storage, p->aa_pad, p->row_stride, p->row_origin,
         reinterpret_cast<float2*>(p->traces));
     LAUNCH_CHECK("aa_integrate_kernel");
     p->traces_loaded = true;
@@ -897,10 +908,10 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
   if (p->params.storage == PSTM_F32) {
     if (trace_major)
       stage_rows_x2_kernel<<<(unsigned)n, 256, 0, s>>>(traces, n, n_s, p->perm, p->row_stride,
-                                                       (float2*)p->traces);
+                                                       p->row_origin, (float2*)p->traces);
     else
       stage_transpose_x2_kernel<<<tg, tb, 0, s>>>(traces, n, n_s, p->inv_perm, p->row_stride,
-                                                  (float2*)p->traces);
+                                                  p->row_origin, (float2*)p->traces);
   } else if (p->params.storage == PSTM_BF16) {
     PSTM_STAGE(__nv_bfloat16)
   } else {
