@@ -15,13 +15,85 @@ Python loop (views/migration_monitor_dialog.py:201-430).
 from __future__ import annotations
 
 import ctypes as C
-from typing import List, Optional, Sequence, Tuple
+from dataclasses import dataclass, field
+from typing import Any, Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 import torch
 
 from . import _lib
 from .kirchhoff import PSTMPlan, velocity_strides
+
+
+@dataclass
+class OffsetAzimuthBin:
+    """One offset/azimuth class, as the reference's binning table defines it
+    (models/binning.py:34-60): offsets in [offset_min, offset_max), azimuths in
+    [azimuth_min, azimuth_max) degrees clockwise from north, wrapping through
+    360 when azimuth_max < azimuth_min."""
+    name: str
+    offset_min: float
+    offset_max: float
+    azimuth_min: float = 0.0
+    azimuth_max: float = 360.0
+    enabled: bool = True
+    metadata: Dict[str, Any] = field(default_factory=dict)
+
+    def __post_init__(self):
+        if self.offset_min < 0 or self.offset_max <= self.offset_min:
+            raise ValueError(f"bin {self.name}: need 0 <= offset_min < offset_max")
+        if not (0.0 <= self.azimuth_min <= 360.0 and 0.0 <= self.azimuth_max <= 360.0):
+            raise ValueError(f"bin {self.name}: azimuths must lie in [0, 360]")
+
+
+def offset_azimuth(source_x: torch.Tensor, source_y: torch.Tensor, receiver_x: torch.Tensor,
+                   receiver_y: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Offset (float32, m) and source-to-receiver azimuth (degrees in [0, 360),
+    clockwise from north) on the coordinates' device, in the coordinates'
+    precision as the reference forms them (models/migration_geometry.py:88-116)."""
+    dx = receiver_x - source_x
+    dy = receiver_y - source_y
+    off = torch.sqrt(dx * dx + dy * dy).to(torch.float32)
+    az = torch.remainder(torch.rad2deg(torch.atan2(dx, dy)) + 360.0, 360.0)
+    return off, az
+
+
+def bin_indices(source_x: torch.Tensor, source_y: torch.Tensor, receiver_x: torch.Tensor,
+                receiver_y: torch.Tensor, bins: Sequence[OffsetAzimuthBin]) -> List[torch.Tensor]:
+    """Trace indices (on the coordinates' device) of every enabled bin.
+
+    The reference assigns traces bin by bin on the host and the worker then
+    migrates bin after bin (models/binning.py:304-325,
+    views/migration_monitor_dialog.py:201-254).  Here the class of each trace is
+    found on the device and one stable sort groups the classes, so the whole
+    binning costs one device-to-host copy of the class sizes.  Bins that
+    overlap are resolved bin by bin instead (a trace may then belong to several).
+    """
+    bins = [b for b in bins if b.enabled]
+    off, az = offset_azimuth(source_x, source_y, receiver_x, receiver_y)
+
+    def member(b):
+        ok = (off >= b.offset_min) & (off < b.offset_max)
+        if b.azimuth_max < b.azimuth_min:
+            return ok & ((az >= b.azimuth_min) | (az < b.azimuth_max))
+        return ok & (az >= b.azimuth_min) & (az < b.azimuth_max)
+
+    masks = [member(b) for b in bins]
+    if not masks:
+        return []
+    count = torch.stack(masks).sum(0)
+    if bool((count > 1).any()):  # overlapping bins
+        return [torch.nonzero(m).flatten() for m in masks]
+    cls = torch.full(off.shape, len(bins), dtype=torch.int64, device=off.device)
+    for i, m in enumerate(masks):
+        cls = torch.where(m, torch.full_like(cls, i), cls)
+    order = torch.argsort(cls, stable=True)
+    sizes = torch.bincount(cls, minlength=len(bins) + 1)[:len(bins)].tolist()
+    out, start = [], 0
+    for n in sizes:
+        out.append(order[start:start + n])
+        start += n
+    return out
 
 
 def class_indices(offset: np.ndarray, azimuth: np.ndarray, n_offset_bins: int,
@@ -73,6 +145,10 @@ class BatchedPSTM:
             self._graph = None
             self._lib.pstm_batch_destroy(self._handle)
             self._handle = C.c_void_p(None)
+        if getattr(self, "_own_plans", False):
+            for p in self.plans:
+                p.close()
+            self._own_plans = False
 
     def __del__(self):
         try:
@@ -91,6 +167,37 @@ class BatchedPSTM:
     def check(self) -> None:
         for p in self.plans:
             p.check()
+
+    # ------------------------------------------------------- from a survey
+    @classmethod
+    def from_survey(cls, traces: torch.Tensor, source_x: torch.Tensor, source_y: torch.Tensor,
+                    receiver_x: torch.Tensor, receiver_y: torch.Tensor,
+                    bins: Sequence[OffsetAzimuthBin], velocity: torch.Tensor,
+                    with_fold: bool = True, **plan_kwargs) -> "BatchedPSTM":
+        """Bins a whole survey on the device and builds one plan per non-empty
+        class (``plan_kwargs`` as for ``PSTMPlan``: grid, axes, aperture ...).
+        ``traces`` (n_samples, n_traces) stay on the device; each class's traces
+        are gathered into ``self.class_traces`` and loaded.  ``self.bins`` and
+        ``self.indices`` name the classes and their traces."""
+        dev = traces.device
+        idx = bin_indices(source_x.to(dev), source_y.to(dev), receiver_x.to(dev),
+                          receiver_y.to(dev), bins)
+        keep = [(b, i) for b, i in zip([b for b in bins if b.enabled], idx) if i.numel() > 0]
+        if not keep:
+            raise ValueError("no trace falls in an enabled bin")
+        plans, class_traces = [], []
+        for _, i in keep:
+            coords = [a.to(dev).index_select(0, i).contiguous()
+                      for a in (source_x, source_y, receiver_x, receiver_y)]
+            plans.append(PSTMPlan(*coords, **plan_kwargs))
+            class_traces.append(traces.index_select(1, i).contiguous())
+        batch = cls(plans, velocity, with_fold=with_fold)
+        batch._own_plans = True
+        batch.bins = [b for b, _ in keep]
+        batch.indices = [i for _, i in keep]
+        batch.class_traces = class_traces
+        batch.load(class_traces)
+        return batch
 
     # ------------------------------------------------------------ CUDA graph
     def capture(self, traces: Sequence[torch.Tensor]) -> None:

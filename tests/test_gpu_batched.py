@@ -88,3 +88,43 @@ def test_autotuner_picks_and_caches(tmp_path, monkeypatch):
     assert autotune.cached_variant(key) == best
     best2, times2 = autotune.tune(make, s.traces.cuda(), v, key, autotune.candidates(s.n_xl))
     assert best2 == best and times2 == {}
+
+
+def test_from_survey_matches_per_class_plans():
+    """A whole survey binned on the device into offset/azimuth classes, one
+    batched launch: each class image equals a plan built from that class's
+    traces selected on the host."""
+    from seisproc_b200 import synthetic
+    from seisproc_b200.batched import BatchedPSTM, OffsetAzimuthBin
+    from seisproc_b200.kirchhoff import PSTMPlan
+    s = synthetic.survey_3d(n_traces=4000, seed=12, n_samples=200, extent=1000.0,
+                            max_offset=1200.0, n_il=10, n_xl=9, spacing=25.0, n_diffractors=6,
+                            aperture=400.0)
+    dev = torch.device("cuda")
+    bins = [OffsetAzimuthBin(f"o{i}a{j}", 400.0 * i, 400.0 * (i + 1), 180.0 * j, 180.0 * (j + 1))
+            for i in range(3) for j in range(2)]
+    kw = dict(n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+              origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0, xl_dy=s.xl_spacing,
+              t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples, in_t0_ms=0.0, in_dt_ms=s.dt_ms,
+              max_aperture_m=s.max_aperture_m, max_angle_deg=s.max_angle_deg)
+    coords = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+              for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    v = torch.from_numpy(s.vrms).to(dev)
+    tr = s.traces.to(dev)
+    b = BatchedPSTM.from_survey(tr, *coords, bins, v, **kw)
+    b.migrate()
+    b.check()
+    off = np.sqrt((s.receiver_x - s.source_x) ** 2 + (s.receiver_y - s.source_y) ** 2)
+    az = (np.degrees(np.arctan2(s.receiver_x - s.source_x, s.receiver_y - s.source_y)) + 360) % 360
+    assert sum(int(i.numel()) for i in b.indices) == s.n_traces
+    for bn, idx, img, fold in zip(b.bins, b.indices, b.images, b.folds):
+        sel = np.nonzero((off >= bn.offset_min) & (off < bn.offset_max) &
+                         (az >= bn.azimuth_min) & (az < bn.azimuth_max))[0]
+        assert np.array_equal(idx.cpu().numpy(), sel)
+        c = [a[torch.from_numpy(sel).to(dev)] for a in coords]
+        p = PSTMPlan(*c, **kw)
+        ri, rf = p.migrate(tr[:, torch.from_numpy(sel).to(dev)], v)
+        p.check()
+        assert torch.equal(img, ri) and torch.equal(fold, rf)
+        p.close()
+    b.close()
