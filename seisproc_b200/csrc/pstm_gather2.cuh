@@ -9,8 +9,9 @@
 // trace: leg distances and the first contributing sample by binary search in
 // the CTA's threshold table), then sweeps the traces, taking each trace's
 // set-up from its lane by shuffle.  Samples are read straight from the staged
-// row: float32 rows hold expanded (x[i], x[i+1] - x[i]) entries (one 8-byte
-// load and one FMA per sample), 16-bit rows plain samples (two loads).
+// row: float32 rows hold expanded entries, each linear piece as intercept and
+// slope in the index frame (one 8-byte load and one FMA per sample), 16-bit
+// rows plain samples (two loads and a lerp).
 #pragma once
 #include "pstm_gather.cuh"
 

@@ -176,3 +176,48 @@ def test_normalize_by_fold_kat():
     assert torch.allclose(n, torch.tensor([[[5.0, 5.0], [10.0, 0.0]]]))
     n2 = normalize_by_fold(torch.tensor([[[10.0, 20.0]]]), torch.tensor([[[1.0, 0.5]]]), 1)
     assert n2[0, 0, 0].item() == 10.0 and n2[0, 0, 1].item() == 20.0
+
+
+def _plan_3d(s, in_t0_ms=0.0, **kw):
+    from seisproc_b200.kirchhoff import PSTMPlan
+    dev = torch.device("cuda")
+    c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    plan = PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+                    origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                    xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                    in_t0_ms=in_t0_ms, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                    max_angle_deg=s.max_angle_deg, **kw)
+    img, fold = plan.migrate(s.traces.cuda(), torch.from_numpy(s.vrms).cuda())
+    plan.check()
+    plan.close()
+    return img.reshape(s.n_times, -1).cpu().numpy(), fold.reshape(s.n_times, -1).cpu().numpy()
+
+
+@pytest.mark.parametrize("weight", ["obliquity_spreading", "spreading", "obliquity", "none"])
+def test_weight_modes_match_fp64_oracle(weight):
+    """Every weight mode (index-scaled and plain traveltime paths) vs FP64."""
+    s = _small_3d(seed=6)
+    img, fold = _plan_3d(s, weight=weight)
+    oi, of = _oracle_3d(s, weight=weight)
+    assert rel_l2(img, oi) <= FP32_TOL, weight
+    assert np.abs(fold - of).sum() <= max(2, FOLD_FLIP_FRAC * of.sum())
+
+
+def test_output_before_first_input_sample():
+    """Input traces starting 40 ms after the output axis: indices below the first
+    sample clamp to it (the low-clamp path), as the reference's clamp to
+    [0, N - 1.001] does (kirchhoff_kernel.py:707-709)."""
+    s = _small_3d(seed=7)
+    img, fold = _plan_3d(s, in_t0_ms=40.0)
+    n_t = s.n_times
+    il = np.arange(s.n_il)[:, None]
+    xl = np.arange(s.n_xl)[None, :]
+    cx = (s.origin_x + il * s.il_spacing + 0 * xl).ravel()
+    cy = (s.origin_y + 0 * il + xl * s.xl_spacing).ravel()
+    t_ms = (np.arange(n_t, dtype=np.float32) * np.float32(s.dt_ms)).astype(np.float64)
+    oi, of = O.migrate_fp64(s.traces.cpu().numpy(), s.source_x, s.source_y, s.receiver_x,
+                            s.receiver_y, cx, cy, t_ms, s.vrms.reshape(n_t, -1), s.dt_ms, 40.0,
+                            s.max_aperture_m, s.max_angle_deg)
+    assert rel_l2(img, oi) <= FP32_TOL
+    assert np.abs(fold - of).sum() <= max(2, FOLD_FLIP_FRAC * of.sum())
