@@ -9,9 +9,10 @@
 // trace: leg distances and the first contributing sample by binary search in
 // the CTA's threshold table), then sweeps the traces, taking each trace's
 // set-up from its lane by shuffle.  Samples are read straight from the staged
-// row: float32 rows hold expanded entries, each linear piece as intercept and
-// slope in the index frame (one 8-byte load and one FMA per sample), 16-bit
-// rows plain samples (two loads and a lerp).
+// row: float32 rows hold expanded (x[i], x[i+1] - x[i]) entries (one 8-byte
+// load per sample), the anti-alias integral rows each linear piece as intercept
+// and slope in the index frame (one load and one FMA per tap), 16-bit rows
+// plain samples (two loads and a lerp).
 #pragma once
 #include "pstm_gather.cuh"
 
@@ -144,11 +145,11 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
       const uint32_t a1 = rbase[n] + (__float_as_uint(tm.y) << SHIFT);
       f2 dx, amp;
       if constexpr (std::is_same<ST, float2>::value) {
-        // expanded rows: one 8-byte load gives the piece's intercept and slope
-        // in the index frame, so the interpolant is one FMA of the index
+        // expanded rows: one 8-byte load gives (x[i0], x[i0+1] - x[i0])
+        const f2 fr = f2_sub(id, f2_sub(tm, magic2));
         const f2 e0 = lds_f2(a0), e1 = lds_f2(a1);
         dx = f2{e0.y, e1.y};
-        amp = f2{fmaf(id.x, e0.y, e0.x), fmaf(id.y, e1.y, e1.x)};
+        amp = f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
       } else {
         const f2 fr = f2_sub(id, f2_sub(tm, magic2));
         const f2 x0 = f2{lds_elem<ST>(a0), lds_elem<ST>(a1)};
@@ -372,15 +373,15 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     }
     acc[i] = f2{0.f, 0.f};
   }
-  // Index frame of the sweeps.  16-bit rows: the staged position idx - lo.
-  // Expanded rows (sample i at entry i + 1, or i + pad for the anti-alias
-  // integral): the entry coordinate less the rows' intercept origin q0; the
-  // rounding-down add of 2^23 + q0 - lo then yields the staged entry's index
-  // in the float's low bits.
+  // Index frame of the sweeps: the staged position idx - lo (16-bit rows), or
+  // idx + 1 - lo (expanded float32 rows, sample i at entry i + 1).  For the
+  // anti-alias integral (sample i at entry i + pad, intercept form) the entry
+  // coordinate less the rows' intercept origin q0, with the rounding-down add
+  // of 2^23 + q0 - lo yielding the staged entry's index in the float's bits.
   constexpr bool kExpanded = std::is_same<ST, float2>::value;
-  const float shift = kExpanded ? (AA ? (float)A.aa_pad : 1.0f) - (float)A.row_origin
-                                : -(float)lo;
-  const f2 mg = f2_bcast(kExpanded ? kMagic + (float)(A.row_origin - lo) : kMagic);
+  const float shift = AA ? (float)A.aa_pad - (float)A.row_origin
+                        : (kExpanded ? 1.0f : 0.0f) - (float)lo;
+  const f2 mg = f2_bcast(AA ? kMagic + (float)(A.row_origin - lo) : kMagic);
   const float bconst = -A.in_t0 / A.in_dt + shift;
   const f2 bb = f2_bcast(bconst);
   const float hi_c = A.clamp_hi + shift;

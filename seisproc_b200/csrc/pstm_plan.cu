@@ -336,10 +336,14 @@ __device__ __forceinline__ float2 expanded_entry(float x0, float x1, int q, int 
   return make_float2((float)((double)x0 - (double)(q - q0) * (double)d), d);
 }
 
-// float32 staging into expanded entries at row position i + 1 (x = 0 outside
-// the trace), sample-major input via 33 x 32 shared tiles.
+// float32 staging into (x[i], x[i+1] - x[i]) entries at row position i + 1
+// (x = 0 outside the trace), sample-major input via 33 x 32 shared tiles.  The
+// plain operator keeps this sample-and-step form: its interpolant
+// x + f (x' - x) rounds like the adjoint's transposed split, which keeps the
+// dot-product test of the pair at float32 rounding (the intercept form below
+// would add ~1e-5 on white-noise data).
 __global__ void stage_transpose_x2_kernel(const float* tr, int64_t n_tr, int n_s,
-                                          const int* inv_perm, int S, int q0, float2* out) {
+                                          const int* inv_perm, int S, float2* out) {
   __shared__ float tile[33][33];
   const int64_t j0 = (int64_t)blockIdx.x * 32;
   const int i0 = blockIdx.y * 32;
@@ -355,20 +359,20 @@ __global__ void stage_transpose_x2_kernel(const float* tr, int64_t n_tr, int n_s
     if (j < n_tr && i < n_s) {
       const int jj = inv_perm[j];
       const float x0 = tile[threadIdx.x][r], x1 = tile[threadIdx.x + 1][r];
-      out[(int64_t)jj * S + i + 1] = expanded_entry(x0, x1, i + 1, q0);
-      if (i == 0) out[(int64_t)jj * S] = expanded_entry(0.f, x0, 0, q0);
+      out[(int64_t)jj * S + i + 1] = make_float2(x0, x1 - x0);
+      if (i == 0) out[(int64_t)jj * S] = make_float2(0.f, x0);
     }
   }
 }
 
 __global__ void stage_rows_x2_kernel(const float* tr, int64_t n_tr, int n_s, const int* perm,
-                                     int S, int q0, float2* out) {
+                                     int S, float2* out) {
   const int64_t jj = blockIdx.x;
   const float* x = tr + (int64_t)perm[jj] * n_s;
   for (int i = (int)threadIdx.x - 1; i < n_s; i += blockDim.x) {
     const float x0 = i >= 0 ? x[i] : 0.f;
     const float x1 = i + 1 < n_s ? x[i + 1] : 0.f;
-    out[jj * S + i + 1] = expanded_entry(x0, x1, i + 1, q0);
+    out[jj * S + i + 1] = make_float2(x0, x1 - x0);
   }
 }
 
@@ -677,7 +681,6 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
     // (x[i], x[i+1] - x[i]) entries for i = -1 .. N-1 at row positions i + 1
     p->row_stride = (int)align_up(prm->n_samples + 1, 8);
     p->elt_bytes = 8;
-    p->row_origin = (prm->n_samples + 1) / 2;
   }
   if (prm->antialias) {
     // rows hold the trend-removed double integral I2[-pad .. N + pad] in float32
@@ -908,10 +911,10 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
   if (p->params.storage == PSTM_F32) {
     if (trace_major)
       stage_rows_x2_kernel<<<(unsigned)n, 256, 0, s>>>(traces, n, n_s, p->perm, p->row_stride,
-                                                       p->row_origin, (float2*)p->traces);
+                                                       (float2*)p->traces);
     else
       stage_transpose_x2_kernel<<<tg, tb, 0, s>>>(traces, n, n_s, p->inv_perm, p->row_stride,
-                                                  p->row_origin, (float2*)p->traces);
+                                                  (float2*)p->traces);
   } else if (p->params.storage == PSTM_BF16) {
     PSTM_STAGE(__nv_bfloat16)
   } else {

@@ -48,6 +48,29 @@ def test_dot_product_test():
     assert rel <= 1e-5, (a, b, rel)
 
 
+def test_dot_product_test_least_squares_size():
+    """The least-squares workload's geometry at a quarter of its traces (500
+    samples at 2 ms, 100 x 100 grid, 1000 m aperture), white-noise m and d: the
+    worst case for float32 rounding differences between the two operators."""
+    from seisproc_b200 import synthetic
+    from seisproc_b200.autograd import dot_product_test
+    from seisproc_b200.kirchhoff import PSTMPlan
+    s = synthetic.survey_3d(n_traces=30_000, seed=7, n_samples=500, dt_ms=2.0, extent=2500.0,
+                            max_offset=1500.0, n_il=100, n_xl=100, spacing=25.0,
+                            n_diffractors=10, aperture=1000.0)
+    dev = torch.device("cuda")
+    c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    plan = PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+                    origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                    xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                    in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                    max_angle_deg=s.max_angle_deg)
+    a, b, rel = dot_product_test(plan, torch.from_numpy(s.vrms).to(dev), seed=7)
+    plan.close()
+    assert rel <= 1e-5, (a, b, rel)
+
+
 def test_demigration_matches_fp64_oracle():
     s = _survey(seed=12)
     plan = _plan(s)
