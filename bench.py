@@ -9,7 +9,7 @@ aperture, 60 deg angle.  Synthetic, seeded.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|bf16|f16]
                   [--antialias] [--utm]
   python bench.py --impl reference ...   (CPU port of the reference kernel)
-  python bench.py --config batched | lsq
+  python bench.py --config batched | lsq | velocity
 
 ``--antialias --utm --storage bf16|f16`` is the anti-aliased workload with
 traces stored in 16 bits and world coordinates offset by a UTM origin.  Every
@@ -572,6 +572,92 @@ def bench_lsq(args):
     plan.close()
 
 
+def bench_velocity(args):
+    """V_rms ingestion: a picked 3-D velocity cube (coarse nodes, as an
+    IL-XL-T-V or SEG-Y velocity file gives) resampled onto every sample of the
+    3D output grid (1000 x 200 x 200) by pstm_velocity_grid.  value = output
+    samples per second of the kernel with the model and tables resident;
+    roofline = its 4 written bytes per sample against HBM; e2e = the whole
+    velocity_grid() call (host tables, uploads, kernel); cpu_baseline = the
+    float64 numpy restatement on a column sample."""
+    from seisproc_b200 import _lib
+    from seisproc_b200 import models as M
+    from seisproc_b200.velocity_io import VelocityGridder, velocity_grid
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    L = _lib.lib()
+    n_t, n = args.samples, args.grid
+    rs = np.random.RandomState(5)
+    z = np.linspace(0.0, 4.2, 43).astype(np.float32)          # picks every 100 ms
+    x = np.linspace(-250.0, 5250.0, 23).astype(np.float32)    # nodes every 250 m
+    y = np.linspace(-250.0, 5250.0, 23).astype(np.float32)
+    cube = (1500 + 500 * z[:, None, None] + 0.02 * x[None, :, None] + 0.01 * y[None, None, :]
+            + rs.uniform(-25, 25, (z.size, x.size, y.size))).astype(np.float32)
+    m = M.create_3d_velocity(cube, z, x, y)
+    t_s = np.arange(n_t) * 0.004
+    il = np.arange(n)[:, None]
+    xl = np.arange(n)[None, :]
+    cx = (12.5 + 25.0 * il + 0 * xl).ravel()
+    cy = (12.5 + 0 * il + 25.0 * xl).ravel()
+    g = VelocityGridder(m, t_s, cx, cy, dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > L2
+    for _ in range(args.warmup):
+        g.run()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    l0 = L.pstm_launch_count()
+    with ClockSampler(0) as clk:
+        for a, b in ev:
+            flush.zero_()
+            a.record()
+            g.run()
+            b.record()
+        torch.cuda.synchronize()
+    launches = L.pstm_launch_count() - l0
+    ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+    samples = float(n_t * n * n)
+    # e2e: the public call, host tables + uploads + kernel + D2H of the grid
+    e2e_ms = []
+    for _ in range(max(3, min(args.steps, 5))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = velocity_grid(m, t_s, cx, cy, dev).cpu()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e = statistics.median(e2e_ms)
+    ok = np.array_equal(out.numpy(), g.out.cpu().numpy())
+    # CPU: the float64 numpy restatement on every 50th column
+    sel = np.arange(0, n * n, 50)
+    t0 = time.perf_counter()
+    host = m.rms_grid(t_s, cx[sel], cy[sel])
+    cpu_s = time.perf_counter() - t0
+    dv = g.out.cpu().numpy()[:, sel]
+    ulps = int(np.abs(dv.view(np.int32).astype(np.int64) -
+                      host.view(np.int32).astype(np.int64)).max())
+    pk = peaks()
+    gbs = samples * 4 / (ms * 1e-3) / 1e9
+    print(json.dumps({
+        "metric": "V_rms grid Gsamples/s", "value": samples / (ms * 1e-3) / 1e9,
+        "unit": "Gsamples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 blend, f32 out", "data": "synthetic",
+        "config": {"workload": f"3-D velocity cube {z.size}x{x.size}x{y.size} nodes resampled "
+                               f"onto the {n}x{n}x{n_t} output grid",
+                   "l2": "256 MB buffer written between timed launches"},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": gbs / pk["hbm_gbs"], "traffic": None,
+                     "algorithmic_bytes_per_sample": 4, "peak_source": pk["source"]},
+        "e2e": {"value": samples / (e2e * 1e-3) / 1e9, "unit": "Gsamples/s",
+                "h2d_bytes_per_step": int(cube.nbytes + 12 * n_t + 24 * n * n),
+                "d2h_bytes_per_step": int(samples * 4), "ms_per_step": e2e,
+                "matches_resident_run": ok},
+        "cpu_baseline": {"value": sel.size * n_t / cpu_s / 1e9, "unit": "Gsamples/s", "cores": 1,
+                         "kind": "port", "sample": f"{sel.size} of {n * n} columns x {n_t} "
+                                                   "times, float64 numpy"},
+        "max_ulps_vs_host": ulps, "gpu_launches": int(launches), "clocks": clk.summary(),
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -596,12 +682,14 @@ def main():
     ap.add_argument("--lsq-traces", type=int, default=120_000)
     ap.add_argument("--cg-iters", type=int, default=10)
     ap.add_argument("--fd-directions", type=int, default=20)
-    ap.add_argument("--config", default="3d", choices=["3d", "batched", "lsq"])
+    ap.add_argument("--config", default="3d", choices=["3d", "batched", "lsq", "velocity"])
     args = ap.parse_args()
     if args.config == "batched" and args.impl == "ours":
         return bench_batched(args)
     if args.config == "lsq" and args.impl == "ours":
         return bench_lsq(args)
+    if args.config == "velocity" and args.impl == "ours":
+        return bench_velocity(args)
     if args.impl == "reference":
         bench_reference(args)
     else:

@@ -199,6 +199,25 @@ pstm_status pstm_normalize_by_fold(const float* image, const float* fold, float*
 pstm_status pstm_normalize_mute(const float* image, const float* fold, float* out, int64_t n,
                                 float min_fold, void* stream);
 
+/* ---- velocity ingestion ------------------------------------------------- */
+
+/* V_rms at every output sample, out[k * n_cols + c] (float32), resampled on the
+ * device from a velocity model `model` laid out (nz, nx, ny) C-order float32 on
+ * its own (time, x, y) axes.  It replaces the point-by-point scipy evaluation
+ * of models/velocity_model.py:181-245 (RegularGridInterpolator, linear,
+ * fill_value=None: linear extrapolation beyond the axis ends) for the 2-D and
+ * 3-D models that utils/velocity_io.py:1007-1173 reads.  The per-axis tables
+ * come from the host: for output time k, iz[k] is the model interval
+ * (clamped to [0, nz - 2]) and wz[k] the fraction within it (outside [0, 1]
+ * when extrapolating); ix/wx and iy/wy likewise per output column.  A 2-D
+ * model passes ny = 1 and iy = wy = NULL.  An axis of length 1 is constant
+ * along it.  All pointers are device pointers; the blend is float64, rounded
+ * once to float32. */
+pstm_status pstm_velocity_grid(const float* model, int32_t nz, int32_t nx, int32_t ny,
+                               const int32_t* iz, const double* wz, int32_t n_t,
+                               const int32_t* ix, const double* wx, const int32_t* iy,
+                               const double* wy, int64_t n_cols, float* out, void* stream);
+
 /* ---- batched migration: many plans in one persistent launch ------------- */
 typedef struct pstm_batch pstm_batch;
 

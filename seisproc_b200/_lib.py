@@ -89,6 +89,8 @@ _SIGNATURES = {
     "pstm_batch_migrate": (C.c_int, [_P, _P]),
     "pstm_batch_destroy": (C.c_int, [_P]),
     "pstm_batch_size": (C.c_int32, [_P]),
+    "pstm_velocity_grid": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, C.c_int32,
+                                     _P, _P, _P, _P, C.c_int64, _P, _P]),
     "pstm_migrate_noalloc": (C.c_int, [C.POINTER(Grid), C.POINTER(Params), C.POINTER(Geometry),
                                        _P, _P, C.c_int64, C.c_int64, _P, _P, _P]),
 }

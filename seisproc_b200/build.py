@@ -26,6 +26,7 @@ SOURCES = [
     "pstm_gather_vgrad.cu",
     "pstm_noalloc.cu",
     "pstm_batch.cu",
+    "pstm_velocity.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -29,6 +29,7 @@ from .kernel_backend import require_cuda
 from .kirchhoff import PSTMPlan
 from . import models as _models
 from . import velocity as _velocity
+from .velocity_io import velocity_grid
 
 logger = logging.getLogger(__name__)
 
@@ -128,8 +129,15 @@ class MigrationEngine:
             xl = np.arange(n_xl)[None, :]
             col_x = (origin_x + il * il_spacing + 0 * xl).ravel()
             col_y = (origin_y + 0 * il + xl * xl_spacing).ravel()
-            vel = velocity_at_outputs(velocity_mps, velocity_model, t_ms, col_x, col_y)
-            vel_t = torch.from_numpy(np.ascontiguousarray(vel)).to(self.device)
+            if isinstance(velocity_model, _models.VelocityModel) and \
+                    velocity_model.velocity_type in (_models.VelocityType.V_OF_XZ,
+                                                     _models.VelocityType.V_OF_XYZ):
+                # laterally varying: resampled onto the output grid on the device
+                vel_t = velocity_grid(velocity_model, np.asarray(t_ms, np.float64) / 1000.0,
+                                      col_x, col_y, self.device)
+            else:
+                vel = velocity_at_outputs(velocity_mps, velocity_model, t_ms, col_x, col_y)
+                vel_t = torch.from_numpy(np.ascontiguousarray(vel)).to(self.device)
             plan = PSTMPlan(*coords, n_il=n_il, n_xl=n_xl, n_times=n_t, origin_x=origin_x,
                             origin_y=origin_y, il_dx=il_spacing, il_dy=0.0, xl_dx=0.0,
                             xl_dy=xl_spacing, t0_ms=t_min_ms, dt_ms=dt_ms, n_samples=n_s,

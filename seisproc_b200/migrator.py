@@ -196,12 +196,16 @@ class KirchhoffMigrator(BaseMigrator):
         y = (g.y_origin + 0 * il + xl * g.d_xline).ravel()
         return x, y
 
-    def _velocity_grid(self) -> np.ndarray:
+    def _velocity_grid(self) -> torch.Tensor:
+        """V at the output samples on the device (laterally varying models are
+        resampled there by ``velocity_io.velocity_grid``)."""
+        from .velocity_io import velocity_grid
         g = self.config.output_grid
         if self.velocity.is_constant:
-            return np.array([self.velocity.v0], np.float32)
+            return torch.full((1,), float(self.velocity.v0), dtype=torch.float32,
+                              device=self.device)
         cx, cy = self._columns()
-        return self.velocity.rms_grid(g.time_axis, cx, cy)
+        return velocity_grid(self.velocity, g.time_axis, cx, cy, self.device)
 
     def migrate_gather(self, gather: SeismicData, geometry: MigrationGeometry,
                        output_image: Optional[torch.Tensor] = None,
@@ -236,7 +240,7 @@ class KirchhoffMigrator(BaseMigrator):
                 antialias=self.antialias, aa_dx=g.d_inline, aa_dy=g.d_xline,
                 aa_max_halfwidth=self.aa_max_halfwidth)
             try:
-                v = torch.from_numpy(np.ascontiguousarray(self._velocity_grid())).to(self.device)
+                v = self._velocity_grid()
                 tr = torch.from_numpy(np.ascontiguousarray(traces, dtype=np.float32))
                 img, fold = plan.migrate(tr.to(self.device), v)
                 plan.check()

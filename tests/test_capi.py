@@ -64,3 +64,10 @@ def test_null_arguments_rejected():
     assert L.pstm_normalize_by_fold(None, None, None, 0, 1.0, None) == _lib.PSTM_OK
     assert L.pstm_normalize_by_fold(None, None, None, 5, 1.0, None) == _lib.PSTM_EINVAL
     assert L.pstm_check(None, None) == _lib.PSTM_EINVAL
+    # velocity grid: no model, then a 3-D model without its y tables
+    assert L.pstm_velocity_grid(None, 2, 2, 1, None, None, 0, None, None, None, None, 0, None,
+                                None) == _lib.PSTM_EINVAL
+    one = C.c_void_p(16)  # never dereferenced: validation fails first
+    assert L.pstm_velocity_grid(one, 2, 2, 3, one, one, 4, one, one, None, None, 4, one,
+                                None) == _lib.PSTM_EINVAL
+    assert "pstm_velocity_grid" in _lib.last_error()
