@@ -89,7 +89,10 @@ __device__ __forceinline__ void red_add(uint32_t addr, float v) {
 // Pending contributions of a lane: acc0 to sample `cur`, acc1 to `cur + 1`.
 // The lane's samples are consecutive in k, so their indices mostly repeat or
 // step by one; contributions are merged in registers and a shared-memory add
-// is issued only when the index moves on.
+// is issued only when the index moves on, and only for a non-zero sum (masked
+// samples carry zero weight; adding 0 leaves a float unchanged, so skipping it
+// changes no result and saves the compare-and-swap loop a float add to shared
+// memory compiles to).
 struct AdjRun {
   uint32_t cur;  // address of sample cur
   float acc0, acc1;
@@ -98,8 +101,8 @@ struct AdjRun {
 __device__ __forceinline__ void adj_push(AdjRun& r, uint32_t a, float g0, float g1) {
   const bool same = a == r.cur;
   const bool next = a == r.cur + 4;
-  if (!same) red_add(r.cur, r.acc0);
-  if (!same && !next) red_add(r.cur + 4, r.acc1);
+  if (!same && r.acc0 != 0.f) red_add(r.cur, r.acc0);
+  if (!same && !next && r.acc1 != 0.f) red_add(r.cur + 4, r.acc1);
   r.acc0 = same ? r.acc0 + g0 : (next ? r.acc1 + g0 : g0);
   r.acc1 = same ? r.acc1 + g1 : g1;
   r.cur = a;
@@ -168,8 +171,8 @@ __device__ __forceinline__ void adj_sweep(const f2 (&zz)[M], const f2 (&aa)[M], 
     }
     adj_push(run, a1, g0v.y, g1.y);
   }
-  red_add(run.cur, run.acc0);
-  red_add(run.cur + 4, run.acc1);
+  if (run.acc0 != 0.f) red_add(run.cur, run.acc0);
+  if (run.acc1 != 0.f) red_add(run.cur + 4, run.acc1);
 }
 
 // Lane l of warp (column, segment ts) takes the 2M consecutive samples of
@@ -177,8 +180,8 @@ __device__ __forceinline__ void adj_sweep(const f2 (&zz)[M], const f2 (&aa)[M], 
 // shares of shallow and deep samples), and the lanes of one scatter are 2M
 // samples apart, so they rarely hit the same trace sample.  Warps visit the
 // CTA's traces in rotated order, so two warps rarely update one row at once.
-template <int COLS, int WPC, int M, int WM, bool LOWC>
-__global__ void __launch_bounds__(COLS* WPC * 32, 1)
+template <int COLS, int WPC, int M, int WM, bool LOWC, int MINB>
+__global__ void __launch_bounds__(COLS* WPC * 32, MINB)
     pstm_adjoint_kernel(const KArgs A, const float4* __restrict__ tab,
                         const int64_t* __restrict__ blk_off, const int* __restrict__ blk_tiles,
                         int64_t n_traces, int n_windows, int tb) {
@@ -256,32 +259,35 @@ __global__ void __launch_bounds__(COLS* WPC * 32, 1)
   }
 }
 
-template <int COLS, int WPC, int M, int WM>
+template <int COLS, int WPC, int M, int WM, int MINB>
 cudaError_t adj_launch(const Plan* p, const KArgs& A, const float4* tab, cudaStream_t s) {
-  auto kern = needs_lowclamp(p) ? pstm_adjoint_kernel<COLS, WPC, M, WM, true>
-                                : pstm_adjoint_kernel<COLS, WPC, M, WM, false>;
+  auto kern = needs_lowclamp(p) ? pstm_adjoint_kernel<COLS, WPC, M, WM, true, MINB>
+                                : pstm_adjoint_kernel<COLS, WPC, M, WM, false, MINB>;
   const int tb = p->adj_tb;
+  const int T = WPC * 64 * M;  // output samples per window of this kernel shape
+  const int n_windows = (p->grid.n_times + T - 1) / T;
   const int smem = tb * (p->row_stride + 8) * (int)sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   const int64_t nb = (p->n_traces + tb - 1) / tb;
   kern<<<(unsigned)nb, COLS * WPC * 32, smem, s>>>(A, tab, p->adj_off, p->adj_tiles, p->n_traces,
-                                                  p->n_windows, tb);
+                                                  n_windows, tb);
   count_launch();
   return cudaGetLastError();
 }
 
-template <int COLS, int WPC, int M>
+// MINB: CTAs per SM the register budget is sized for.
+template <int COLS, int WPC, int M, int MINB = 1>
 cudaError_t adj_wm(const Plan* p, const KArgs& A, const float4* tab, cudaStream_t s) {
   switch (p->params.weight) {
     case W_OBL_SPREAD:
-      return adj_launch<COLS, WPC, M, W_OBL_SPREAD>(p, A, tab, s);
+      return adj_launch<COLS, WPC, M, W_OBL_SPREAD, MINB>(p, A, tab, s);
     case W_SPREAD:
-      return adj_launch<COLS, WPC, M, W_SPREAD>(p, A, tab, s);
+      return adj_launch<COLS, WPC, M, W_SPREAD, MINB>(p, A, tab, s);
     case W_OBL:
-      return adj_launch<COLS, WPC, M, W_OBL>(p, A, tab, s);
+      return adj_launch<COLS, WPC, M, W_OBL, MINB>(p, A, tab, s);
     case W_NONE:
-      return adj_launch<COLS, WPC, M, W_NONE>(p, A, tab, s);
+      return adj_launch<COLS, WPC, M, W_NONE, MINB>(p, A, tab, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -301,7 +307,10 @@ cudaError_t adj_dispatch(const Plan* p, const KArgs& A, const float4* tab, cudaS
       return adj_wm<2, 4, 2>(p, A, tab, s);
     case 3:
     case 9:
-      return adj_wm<16, 1, 8>(p, A, tab, s);
+      // 8 samples per lane (256-sample windows) at 64 registers, two CTAs
+      // (32 warps) per SM to hide the latency of the shared-memory adds:
+      // 1.25x faster than 16 samples per lane at 128 registers, one CTA per SM
+      return adj_wm<16, 1, 4, 2>(p, A, tab, s);
   }
   return cudaErrorInvalidValue;
 }
