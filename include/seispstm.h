@@ -140,6 +140,14 @@ pstm_status pstm_plan_destroy(pstm_plan* plan);
 
 pstm_status pstm_plan_get_stats(const pstm_plan* plan, pstm_plan_stats* stats);
 
+/* Plans take their device memory from a stream-ordered pool per device, which
+ * keeps up to 16 GiB of freed memory mapped so that the next plan reuses it
+ * (building and destroying plans per bin then maps nothing new).  This returns
+ * the current device's pooled memory beyond keep_bytes to the driver.  No
+ * counterpart in the reference (its buffers are torch tensors, cached by
+ * torch's allocator; torch.cuda.empty_cache is the analogue). */
+pstm_status pstm_trim_memory(int64_t keep_bytes);
+
 /* Loads traces into the plan's spatially sorted, trace-major device copy in the
  * plan's storage dtype (per-trace float32 scale for BF16/F16; for the
  * anti-alias filter, the trend-removed double integral).  `traces` is

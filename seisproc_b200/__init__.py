@@ -17,7 +17,15 @@ __all__ = [
     "VelocityModel", "VelocityType", "WeightMode", "InterpolationMode", "TraveltimeMode",
     "create_3d_velocity", "create_constant_velocity", "create_from_rms_velocity",
     "MigrationEngine", "migrate_kirchhoff_full", "normalize_by_fold", "PSTMPlan",
+    "release_cached_memory",
 ]
+
+
+def release_cached_memory(keep_bytes: int = 0) -> None:
+    """Return the device memory that finished plans left in the library's pool
+    (beyond ``keep_bytes``) on the current CUDA device to the driver."""
+    from . import _lib
+    _lib.check(_lib.lib().pstm_trim_memory(int(keep_bytes)))
 
 
 def __getattr__(name):

@@ -335,22 +335,23 @@ cudaError_t build_block_lists(Plan* p, cudaStream_t s) {
   void* tmp = nullptr;
   struct Free {
     void** ptrs[4];
+    cudaStream_t s;
     ~Free() {
-      for (auto pp : ptrs)
-        if (*pp) cudaFree(*pp);
+      for (auto pp : ptrs) dev_free(*pp, s);
     }
-  } fr{{(void**)&keys, (void**)&sorted, (void**)&n_sel, &tmp}};
+  } fr{{(void**)&keys, (void**)&sorted, (void**)&n_sel, &tmp}, s};
   cudaError_t e;
-  if ((e = cudaMalloc(&p->adj_off, (nb + 1) * sizeof(int64_t))) != cudaSuccess) return e;
+  if ((e = dev_malloc((void**)&p->adj_off, (nb + 1) * sizeof(int64_t), s)) != cudaSuccess)
+    return e;
   p->bytes += (nb + 1) * sizeof(int64_t);
   if (E == 0) {
     p->n_adj_tiles = 0;
     return cudaMemsetAsync(p->adj_off, 0, (nb + 1) * sizeof(int64_t), s);
   }
   if (E > INT32_MAX) return cudaErrorInvalidValue;
-  if ((e = cudaMalloc(&keys, E * sizeof(uint64_t))) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&sorted, E * sizeof(uint64_t))) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&n_sel, sizeof(int64_t))) != cudaSuccess) return e;
+  if ((e = dev_malloc((void**)&keys, E * sizeof(uint64_t), s)) != cudaSuccess) return e;
+  if ((e = dev_malloc((void**)&sorted, E * sizeof(uint64_t), s)) != cudaSuccess) return e;
+  if ((e = dev_malloc((void**)&n_sel, sizeof(int64_t), s)) != cudaSuccess) return e;
   adj_pair_kernel<<<(unsigned)p->n_tiles, 256, 0, s>>>(p->tile_off, p->tile_list, tb, keys);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   int end_bit = 32;
@@ -360,7 +361,7 @@ cudaError_t build_block_lists(Plan* p, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   e = cub::DeviceSelect::Unique(nullptr, uniq_bytes, sorted, keys, n_sel, (int)E, s);
   if (e != cudaSuccess) return e;
-  if ((e = cudaMalloc(&tmp, std::max(sort_bytes, uniq_bytes))) != cudaSuccess) return e;
+  if ((e = dev_malloc(&tmp, std::max(sort_bytes, uniq_bytes), s)) != cudaSuccess) return e;
   e = cub::DeviceRadixSort::SortKeys(tmp, sort_bytes, keys, sorted, (int)E, 0, end_bit, s);
   if (e != cudaSuccess) return e;
   e = cub::DeviceSelect::Unique(tmp, uniq_bytes, sorted, keys, n_sel, (int)E, s);
@@ -369,7 +370,8 @@ cudaError_t build_block_lists(Plan* p, cudaStream_t s) {
   e = cudaMemcpyAsync(&n_uniq, n_sel, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
-  if ((e = cudaMalloc(&p->adj_tiles, std::max<int64_t>(n_uniq, 1) * sizeof(int))) != cudaSuccess)
+  if ((e = dev_malloc((void**)&p->adj_tiles, std::max<int64_t>(n_uniq, 1) * sizeof(int), s)) !=
+      cudaSuccess)
     return e;
   p->bytes += std::max<int64_t>(n_uniq, 1) * sizeof(int);
   p->n_adj_tiles = n_uniq;
@@ -389,8 +391,8 @@ pstm_status launch_adjoint(Plan* p, const float* image, const float* vel, int64_
   if (!p->adj_off) {
     e = build_block_lists(p, s);
     if (e != cudaSuccess) {
-      cudaFree(p->adj_off);
-      cudaFree(p->adj_tiles);
+      dev_free(p->adj_off, s);
+      dev_free(p->adj_tiles, s);
       p->adj_off = nullptr;
       p->adj_tiles = nullptr;
       return cuda_fail(e, "adjoint trace-block lists", why);
@@ -398,7 +400,7 @@ pstm_status launch_adjoint(Plan* p, const float* image, const float* vel, int64_
   }
   const size_t tab_elems = (size_t)p->grid.n_times * p->grid.n_il * p->grid.n_xl;
   if (!p->adj_table) {
-    e = cudaMalloc(&p->adj_table, tab_elems * sizeof(float4));
+    e = dev_malloc((void**)&p->adj_table, tab_elems * sizeof(float4), s);
     if (e != cudaSuccess) {
       p->adj_table = nullptr;
       return cuda_fail(e, "adjoint column table", why);

@@ -77,6 +77,12 @@ pstm_status launch_velocity_check(Plan* p, const float* vel, int64_t vst, int64_
 bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out);
 size_t forward_smem_bytes(const Plan* p);
 void count_launch();
+// Device memory of plans and their temporaries: stream-ordered allocations from
+// a library pool per device that keeps up to kPoolKeepBytes of freed memory
+// mapped for the next plan (pstm_trim_memory returns it).
+constexpr uint64_t kPoolKeepBytes = uint64_t(16) << 30;
+cudaError_t dev_malloc(void** ptr, size_t bytes, cudaStream_t s);
+void dev_free(void* ptr, cudaStream_t s);
 void set_last_error(const std::string& msg);  // message returned by pstm_last_error
 pstm_status ensure_trace_storage(Plan* p, cudaStream_t s);  // staged rows allocated once
 

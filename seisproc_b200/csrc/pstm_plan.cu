@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -506,10 +507,48 @@ __global__ void normalize_kernel(const float* image, const float* fold, float* o
 
 static int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
+// One pool per device, created on first use.  Freed blocks stay mapped up to
+// kPoolKeepBytes, so a plan built after another one of similar size reuses its
+// memory instead of mapping (and later unmapping) fresh gigabytes.
+static cudaError_t pool_for(int dev, cudaMemPool_t* out) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaError_t e = cudaMemPoolCreate(&pools[dev], &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = kPoolKeepBytes;
+    e = cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+  }
+  *out = pools[dev];
+  return cudaSuccess;
+}
+
+cudaError_t pstm::dev_malloc(void** ptr, size_t bytes, cudaStream_t s) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  cudaMemPool_t pool;
+  if (e == cudaSuccess) e = pool_for(dev, &pool);
+  if (e == cudaSuccess) e = cudaMallocFromPoolAsync(ptr, std::max<size_t>(bytes, 1), pool, s);
+  if (e != cudaSuccess) *ptr = nullptr;
+  return e;
+}
+
+void pstm::dev_free(void* ptr, cudaStream_t s) {
+  if (ptr) cudaFreeAsync(ptr, s);
+}
+
 template <typename T>
-static cudaError_t dalloc(Plan* p, T** ptr, size_t count) {
+static cudaError_t dalloc(Plan* p, T** ptr, size_t count, cudaStream_t s) {
   const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(ptr), bytes);
+  cudaError_t e = dev_malloc(reinterpret_cast<void**>(ptr), bytes, s);
   if (e == cudaSuccess) p->bytes += (int64_t)bytes;
   return e;
 }
@@ -535,15 +574,15 @@ static cudaError_t sort_tile_lists(Plan* p, const TileGeom& tg, cudaStream_t s) 
   size_t tmp_bytes = 0;
   struct Free {
     void** ptrs[5];
+    cudaStream_t s;
     ~Free() {
-      for (auto pp : ptrs)
-        if (*pp) cudaFree(*pp);
+      for (auto pp : ptrs) dev_free(*pp, s);
     }
-  } fr{{(void**)&kin, (void**)&kout, (void**)&vout, (void**)&seg, &tmp}};
-  if ((e = cudaMalloc(&kin, cap * sizeof(uint32_t))) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&kout, cap * sizeof(uint32_t))) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&vout, cap * sizeof(int))) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&seg, (kMaxSegs + 1) * sizeof(int))) != cudaSuccess) return e;
+  } fr{{(void**)&kin, (void**)&kout, (void**)&vout, (void**)&seg, &tmp}, s};
+  if ((e = dev_malloc((void**)&kin, cap * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  if ((e = dev_malloc((void**)&kout, cap * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  if ((e = dev_malloc((void**)&vout, cap * sizeof(int), s)) != cudaSuccess) return e;
+  if ((e = dev_malloc((void**)&seg, (kMaxSegs + 1) * sizeof(int), s)) != cudaSuccess) return e;
   for (int64_t ta = 0; ta < n_tiles;) {
     int64_t tb = ta + 1;
     while (tb < n_tiles && tb - ta < kMaxSegs && off[tb + 1] - off[ta] <= cap) ++tb;
@@ -558,9 +597,9 @@ static cudaError_t sort_tile_lists(Plan* p, const TileGeom& tg, cudaStream_t s) 
                                                     vout, (int)items, nseg, seg, seg + 1, s);
       if (e != cudaSuccess) return e;
       if (need > tmp_bytes) {
-        cudaFree(tmp);
+        dev_free(tmp, s);
         tmp = nullptr;
-        if ((e = cudaMalloc(&tmp, need)) != cudaSuccess) return e;
+        if ((e = dev_malloc(&tmp, need, s)) != cudaSuccess) return e;
         tmp_bytes = need;
       }
       e = cub::DeviceSegmentedSort::StableSortPairs(tmp, tmp_bytes, kin, kout,
@@ -577,20 +616,19 @@ static cudaError_t sort_tile_lists(Plan* p, const TileGeom& tg, cudaStream_t s) 
   return cudaStreamSynchronize(s);
 }
 
+// The plan may have been used on any stream: wait for the device, then
+// return its memory to the pool.
 static void free_plan(Plan* p) {
   if (!p) return;
-  cudaFree(p->geo);
-  cudaFree(p->perm);
-  cudaFree(p->inv_perm);
-  cudaFree(p->tile_off);
-  cudaFree(p->adj_off);
-  cudaFree(p->adj_tiles);
-  cudaFree(p->adj_table);
-  cudaFree(p->tile_list);
-  cudaFree(p->traces);
-  cudaFree(p->scales);
-  cudaFree(p->accum);
-  cudaFree(p->err);
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != p->device) cudaSetDevice(p->device);
+  cudaDeviceSynchronize();
+  void* bufs[] = {p->geo,      p->perm,    p->inv_perm, p->tile_off, p->adj_off, p->adj_tiles,
+                  p->adj_table, p->tile_list, p->traces,  p->scales,   p->accum,   p->err};
+  for (void* b : bufs) dev_free(b, 0);
+  cudaStreamSynchronize(0);
+  if (cur >= 0 && cur != p->device) cudaSetDevice(cur);
   delete p;
 }
 
@@ -629,13 +667,13 @@ static pstm_status validate(const pstm_grid* g, const pstm_params* prm, const ps
 pstm_status pstm::ensure_trace_storage(Plan* p, cudaStream_t s) {
   if (p->traces || p->n_traces == 0) return PSTM_OK;
   const size_t bytes = (size_t)p->n_traces * p->row_stride * p->elt_bytes;
-  CUDA_TRY(cudaMalloc(&p->traces, bytes));
+  CUDA_TRY(dev_malloc(&p->traces, bytes, s));
   p->bytes += (int64_t)bytes;
   CUDA_TRY(cudaMemsetAsync(p->traces, 0, bytes, s));
   // f16 needs a per-trace scale for its range; bf16 has float32's exponent
   // range and is stored unscaled
   if (p->params.storage == PSTM_F16 && !p->params.antialias)
-    CUDA_TRY(dalloc(p, &p->scales, p->n_traces));
+    CUDA_TRY(dalloc(p, &p->scales, p->n_traces, s));
   return PSTM_OK;
 }
 
@@ -705,9 +743,9 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
   if (smem > 227 * 1024)
     return fail(PSTM_EINVAL, "traces too long for the staged kernel (" +
                                  std::to_string(prm->n_samples) + " samples)");
-  CUDA_TRY(dalloc(p, &p->err, 4));
+  CUDA_TRY(dalloc(p, &p->err, 4, s));
   CUDA_TRY(cudaMemsetAsync(p->err, 0, 16, s));
-  CUDA_TRY(dalloc(p, &p->tile_off, p->n_tiles + 1));
+  CUDA_TRY(dalloc(p, &p->tile_off, p->n_tiles + 1, s));
   const int64_t n = p->n_traces;
   if (n == 0) {
     CUDA_TRY(cudaMemsetAsync(p->tile_off, 0, (p->n_tiles + 1) * sizeof(int64_t), s));
@@ -724,21 +762,22 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
   void* cub_tmp = nullptr;
   struct Tmp {
     void** ptrs[9];
+    cudaStream_t s;
     ~Tmp() {
       for (auto pp : ptrs)
-        if (pp && *pp) cudaFree(*pp);
+        if (pp) dev_free(*pp, s);
     }
   } tmp{{(void**)&geo_u, (void**)&mid, (void**)&key, (void**)&key_sorted, (void**)&iota,
-         (void**)&bbox, (void**)&cell_start, (void**)&counts, (void**)&cub_tmp}};
-  CUDA_TRY(cudaMalloc(&geo_u, n * sizeof(float4)));
-  CUDA_TRY(cudaMalloc(&mid, n * sizeof(float2)));
-  CUDA_TRY(cudaMalloc(&key, n * sizeof(int)));
-  CUDA_TRY(cudaMalloc(&key_sorted, n * sizeof(int)));
-  CUDA_TRY(cudaMalloc(&iota, n * sizeof(int)));
-  CUDA_TRY(cudaMalloc(&bbox, 4 * sizeof(int)));
-  CUDA_TRY(dalloc(p, &p->geo, n));
-  CUDA_TRY(dalloc(p, &p->perm, n));
-  CUDA_TRY(dalloc(p, &p->inv_perm, n));
+         (void**)&bbox, (void**)&cell_start, (void**)&counts, (void**)&cub_tmp}, s};
+  CUDA_TRY(dev_malloc((void**)&geo_u, n * sizeof(float4), s));
+  CUDA_TRY(dev_malloc((void**)&mid, n * sizeof(float2), s));
+  CUDA_TRY(dev_malloc((void**)&key, n * sizeof(int), s));
+  CUDA_TRY(dev_malloc((void**)&key_sorted, n * sizeof(int), s));
+  CUDA_TRY(dev_malloc((void**)&iota, n * sizeof(int), s));
+  CUDA_TRY(dev_malloc((void**)&bbox, 4 * sizeof(int), s));
+  CUDA_TRY(dalloc(p, &p->geo, n, s));
+  CUDA_TRY(dalloc(p, &p->perm, n, s));
+  CUDA_TRY(dalloc(p, &p->inv_perm, n, s));
   const int thr = 256;
   const unsigned nblk = (unsigned)((n + thr - 1) / thr);
   if (geo->coord_dtype == PSTM_F64) {
@@ -792,11 +831,11 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
   CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (int64_t*)nullptr,
                                          (int64_t*)nullptr, (int)(p->n_tiles + 1), s));
   tmp_bytes = std::max(tmp_bytes, scan_bytes);
-  CUDA_TRY(cudaMalloc(&cub_tmp, tmp_bytes));
+  CUDA_TRY(dev_malloc(&cub_tmp, tmp_bytes, s));
   CUDA_TRY(cub::DeviceRadixSort::SortPairs(cub_tmp, tmp_bytes, key, key_sorted, iota, p->perm,
                                            (int)n, 0, end_bit, s));
   count_launch();
-  CUDA_TRY(cudaMalloc(&cell_start, (n_cells + 1) * sizeof(int64_t)));
+  CUDA_TRY(dev_malloc((void**)&cell_start, (n_cells + 1) * sizeof(int64_t), s));
   cell_start_kernel<<<(n_cells + 1 + thr - 1) / thr, thr, 0, s>>>(key_sorted, n, n_cells,
                                                                    cell_start);
   LAUNCH_CHECK("cell_start_kernel");
@@ -813,7 +852,7 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
   tg.xl_dx = p->xl_dx;
   tg.xl_dy = p->xl_dy;
   tg.reach = (float)prm->max_aperture_m;
-  CUDA_TRY(cudaMalloc(&counts, (p->n_tiles + 1) * sizeof(int64_t)));
+  CUDA_TRY(dev_malloc((void**)&counts, (p->n_tiles + 1) * sizeof(int64_t), s));
   CUDA_TRY(cudaMemsetAsync(counts, 0, (p->n_tiles + 1) * sizeof(int64_t), s));
   tile_count_kernel<<<(unsigned)p->n_tiles, 256, 0, s>>>(tg, cg, cell_start, p->geo, counts);
   LAUNCH_CHECK("tile_count_kernel");
@@ -825,7 +864,7 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
                            cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   p->list_entries = total;
-  CUDA_TRY(dalloc(p, &p->tile_list, total));
+  CUDA_TRY(dalloc(p, &p->tile_list, total, s));
   if (total > 0) {
     tile_fill_kernel<<<(unsigned)p->n_tiles, 256, 0, s>>>(tg, cg, cell_start, p->geo, p->tile_off,
                                                           p->tile_list);
@@ -840,6 +879,17 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
 
 pstm_status pstm_plan_destroy(pstm_plan* plan) {
   free_plan(reinterpret_cast<Plan*>(plan));
+  return PSTM_OK;
+}
+
+pstm_status pstm_trim_memory(int64_t keep_bytes) {
+  if (keep_bytes < 0) return fail(PSTM_EINVAL, "keep_bytes must be >= 0");
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  CUDA_TRY(pool_for(dev, &pool));
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemPoolTrimTo(pool, (size_t)keep_bytes));
   return PSTM_OK;
 }
 
@@ -876,7 +926,7 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
     // plain float32 rows into the adjoint accumulator (free until demigration),
     // then one warp per row integrates into the staged rows
     const int S_in = (int)align_up(n_s, 8);
-    if (!p->accum) CUDA_TRY(dalloc(p, &p->accum, (size_t)n * p->row_stride));
+    if (!p->accum) CUDA_TRY(dalloc(p, &p->accum, (size_t)n * p->row_stride, s));
     dim3 tb(32, 8);
     dim3 tg((unsigned)((n + 31) / 32), (unsigned)((n_s + 31) / 32));
     if (trace_major)
@@ -980,7 +1030,7 @@ pstm_status pstm_demigrate(pstm_plan* plan, const float* image, const float* vel
   const int n_s = p->n_samples;
   if (n == 0) return PSTM_OK;
   // every sample of every row is written by the adjoint kernel: no clearing
-  if (!p->accum) CUDA_TRY(dalloc(p, &p->accum, (size_t)n * p->row_stride));
+  if (!p->accum) CUDA_TRY(dalloc(p, &p->accum, (size_t)n * p->row_stride, s));
   std::string why;
   st = launch_velocity_check(p, vel, vst, vsc, s, &why);
   if (st != PSTM_OK) return fail(st, why);

@@ -221,3 +221,35 @@ def test_output_before_first_input_sample():
                             s.max_aperture_m, s.max_angle_deg)
     assert rel_l2(img, oi) <= FP32_TOL
     assert np.abs(fold - of).sum() <= max(2, FOLD_FLIP_FRAC * of.sum())
+
+
+def test_plans_reuse_pooled_memory_and_trim():
+    """Plans built and destroyed one after another take their memory from the
+    library's pool; results stay the same, and trimming returns it."""
+    import seisproc_b200
+    from seisproc_b200 import synthetic
+    from seisproc_b200.kirchhoff import PSTMPlan
+    s = synthetic.survey_3d(n_traces=2000, seed=31, n_samples=150, extent=800.0,
+                            max_offset=600.0, n_il=6, n_xl=6, spacing=25.0, n_diffractors=4,
+                            aperture=300.0)
+    dev = torch.device("cuda")
+    c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    v = torch.from_numpy(s.vrms).to(dev)
+    out = []
+    for _ in range(3):
+        p = PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+                     origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                     xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                     in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                     max_angle_deg=s.max_angle_deg)
+        img, fold = p.migrate(s.traces.to(dev), v)
+        p.check()
+        out.append((img.clone(), fold.clone()))
+        p.close()
+    for img, fold in out[1:]:
+        assert torch.equal(img, out[0][0]) and torch.equal(fold, out[0][1])
+    seisproc_b200.release_cached_memory()
+    seisproc_b200.release_cached_memory(1 << 30)
+    with pytest.raises(ValueError):
+        seisproc_b200.release_cached_memory(-1)
