@@ -45,7 +45,7 @@ RSQRT_PER_PAIR = 2
 # DRAM bytes per trace-list entry of the forward gather, from the ncu capture
 # of the 100k-trace case (31.2 GB / 9.0 M entries, 16-column tiles, expanded float32 rows);
 # the traffic of a full launch is scaled by its list entries.
-DRAM_BYTES_PER_LIST_ENTRY = 3473.0
+DRAM_BYTES_PER_LIST_ENTRY = 3470.0
 
 
 def peaks():
@@ -273,7 +273,7 @@ def bench_ours(args):
                     in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
                     max_angle_deg=s.max_angle_deg, storage=args.storage, variant=args.variant,
                     antialias=args.antialias, aa_dx=s.il_spacing, aa_dy=s.xl_spacing,
-                    aa_max_halfwidth=args.aa_lmax)
+                    aa_max_halfwidth=args.aa_lmax, forward_only=True)
     torch.cuda.synchronize()
     t_plan = time.perf_counter() - t_plan
     traces = s.traces

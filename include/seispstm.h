@@ -97,6 +97,12 @@ typedef struct pstm_params {
   double aa_dx, aa_dy;         /* output spacing used for the operator-dip half-width */
   double aa_max_halfwidth;     /* cap on the triangle half-width, in input samples */
   int32_t variant;             /* kernel shape id; 0 = built-in heuristic */
+  int32_t forward_only;        /* 1: the plan only migrates.  float32 rows are then staged in
+                                  intercept form, one FMA per tap and ~3 % faster; the
+                                  demigration stays its transpose to ~1e-5 (not float rounding)
+                                  and pstm_velocity_gradient / batches reject the plan.
+                                  0: (x, dx) rows, migration and demigration an exact float
+                                  transpose pair (dot-product tests, least squares). */
 } pstm_params;
 
 typedef struct pstm_geometry {

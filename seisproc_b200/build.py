@@ -22,6 +22,7 @@ SOURCES = [
     "pstm_plan.cu",
     "pstm_migrate.cu",
     "pstm_gather_fwd.cu",
+    "pstm_gather_fwd_icpt.cu",
     "pstm_adjoint.cu",
     "pstm_gather_vgrad.cu",
     "pstm_noalloc.cu",

@@ -148,6 +148,11 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
       free_batch(b);
       return bfail(PSTM_ENOTSUP, "the batched launch is built for the plain operator");
     }
+    if (p->params.forward_only && p->params.storage == PSTM_F32) {
+      free_batch(b);
+      return bfail(PSTM_ENOTSUP, "the batched launch reads (x, dx) float32 rows: build the "
+                                 "class plans without forward_only");
+    }
     // the descriptors capture the staging buffers, so they must exist now
     const pstm_status st = ensure_trace_storage(p, s);
     if (st != PSTM_OK) {

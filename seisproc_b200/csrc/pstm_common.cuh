@@ -156,6 +156,17 @@ template <>
 struct Storage<float2> {
   static constexpr int kAlign = 2;  // entries per 16 bytes
 };
+// float32 samples expanded into intercept form, for plans that only migrate:
+// entry q holds (x[q-1] - (q - q0) d, d) with d = x[q] - x[q-1] and q0 the
+// plan's row origin, so the interpolant at entry coordinate e is one FMA,
+// (e - q0) d + c
+struct RowIcpt {
+  float c, d;
+};
+template <>
+struct Storage<RowIcpt> {
+  static constexpr int kAlign = 2;  // entries per 16 bytes
+};
 template <>
 struct Storage<__nv_bfloat16> {
   static constexpr int kAlign = 8;

@@ -150,6 +150,11 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
         const f2 e0 = lds_f2(a0), e1 = lds_f2(a1);
         dx = f2{e0.y, e1.y};
         amp = f2{fmaf(fr.x, e0.y, e0.x), fmaf(fr.y, e1.y, e1.x)};
+      } else if constexpr (std::is_same<ST, RowIcpt>::value) {
+        // intercept rows (id is the entry coordinate less q0): one FMA per tap
+        const f2 e0 = lds_f2(a0), e1 = lds_f2(a1);
+        dx = f2{e0.y, e1.y};
+        amp = f2{fmaf(id.x, e0.y, e0.x), fmaf(id.y, e1.y, e1.x)};
       } else {
         const f2 fr = f2_sub(id, f2_sub(tm, magic2));
         const f2 x0 = f2{lds_elem<ST>(a0), lds_elem<ST>(a1)};
@@ -378,10 +383,14 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   // anti-alias integral (sample i at entry i + pad, intercept form) the entry
   // coordinate less the rows' intercept origin q0, with the rounding-down add
   // of 2^23 + q0 - lo yielding the staged entry's index in the float's bits.
-  constexpr bool kExpanded = std::is_same<ST, float2>::value;
+  // Intercept-form float32 rows (sample i at entry i + 1) take the anti-alias
+  // frame with q0 = the plan's row origin.
+  constexpr bool kIcpt = std::is_same<ST, RowIcpt>::value;
+  constexpr bool kExpanded = std::is_same<ST, float2>::value || kIcpt;
   const float shift = AA ? (float)A.aa_pad - (float)A.row_origin
-                        : (kExpanded ? 1.0f : 0.0f) - (float)lo;
-  const f2 mg = f2_bcast(AA ? kMagic + (float)(A.row_origin - lo) : kMagic);
+                     : kIcpt ? 1.0f - (float)A.row_origin
+                             : (kExpanded ? 1.0f : 0.0f) - (float)lo;
+  const f2 mg = f2_bcast(AA || kIcpt ? kMagic + (float)(A.row_origin - lo) : kMagic);
   const float bconst = -A.in_t0 / A.in_dt + shift;
   const f2 bb = f2_bcast(bconst);
   const float hi_c = A.clamp_hi + shift;
@@ -639,7 +648,8 @@ inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
 template <int COLS, int WPC, int M, typename ST, int OP>
 inline cudaError_t dispatch2_wm(const Plan* p, const KArgs& A, cudaStream_t s) {
   const int wm = p->params.weight;
-  constexpr bool k32 = std::is_same<ST, float>::value || std::is_same<ST, float2>::value;
+  constexpr bool k32 = std::is_same<ST, float>::value || std::is_same<ST, float2>::value ||
+                      std::is_same<ST, RowIcpt>::value;
   if constexpr (OP == OP_VGRAD || !k32) {
     if (wm != W_OBL_SPREAD) return cudaErrorNotSupported;
     return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP>(p, A, s);
@@ -658,6 +668,10 @@ inline cudaError_t dispatch2_wm(const Plan* p, const KArgs& A, cudaStream_t s) {
   }
 }
 
+// Forward launch over intercept-form float32 rows (forward_only plans),
+// instantiated in its own translation unit (pstm_gather_fwd_icpt.cu).
+cudaError_t launch_forward_icpt(const Plan* p, const KArgs& A, cudaStream_t s);
+
 template <int COLS, int WPC, int M, int OP>
 inline cudaError_t dispatch2_st(const Plan* p, const KArgs& A, cudaStream_t s) {
   if (p->params.antialias) {
@@ -668,9 +682,16 @@ inline cudaError_t dispatch2_st(const Plan* p, const KArgs& A, cudaStream_t s) {
   }
   switch (p->params.storage) {
     case PSTM_F32:
-      // plans stage expanded (x, dx) rows; the no-allocation path plain rows
-      return p->elt_bytes == 8 ? dispatch2_wm<COLS, WPC, M, float2, OP>(p, A, s)
-                               : dispatch2_wm<COLS, WPC, M, float, OP>(p, A, s);
+      // plans stage expanded (x, dx) rows, forward_only plans intercept-form
+      // rows; the no-allocation path plain rows
+      if (p->elt_bytes != 8) return dispatch2_wm<COLS, WPC, M, float, OP>(p, A, s);
+      if (p->row_origin != 0) {
+        if constexpr (OP == OP_FWD)
+          return launch_forward_icpt(p, A, s);
+        else
+          return cudaErrorNotSupported;
+      }
+      return dispatch2_wm<COLS, WPC, M, float2, OP>(p, A, s);
     case PSTM_BF16:
       return dispatch2_wm<COLS, WPC, M, __nv_bfloat16, OP>(p, A, s);
     case PSTM_F16:

@@ -339,12 +339,17 @@ __device__ __forceinline__ float2 expanded_entry(float x0, float x1, int q, int 
 
 // float32 staging into (x[i], x[i+1] - x[i]) entries at row position i + 1
 // (x = 0 outside the trace), sample-major input via 33 x 32 shared tiles.  The
-// plain operator keeps this sample-and-step form: its interpolant
+// operator keeps this sample-and-step form by default: its interpolant
 // x + f (x' - x) rounds like the adjoint's transposed split, which keeps the
-// dot-product test of the pair at float32 rounding (the intercept form below
-// would add ~1e-5 on white-noise data).
+// dot-product test of the pair at float32 rounding.  Plans that only migrate
+// (q0 > 0) take the intercept form instead (one FMA per tap; against the
+// adjoint it adds ~1e-5 on white-noise data).
+__device__ __forceinline__ float2 row_entry(float x0, float x1, int q, int q0) {
+  return q0 > 0 ? expanded_entry(x0, x1, q, q0) : make_float2(x0, x1 - x0);
+}
+
 __global__ void stage_transpose_x2_kernel(const float* tr, int64_t n_tr, int n_s,
-                                          const int* inv_perm, int S, float2* out) {
+                                          const int* inv_perm, int S, int q0, float2* out) {
   __shared__ float tile[33][33];
   const int64_t j0 = (int64_t)blockIdx.x * 32;
   const int i0 = blockIdx.y * 32;
@@ -360,20 +365,20 @@ __global__ void stage_transpose_x2_kernel(const float* tr, int64_t n_tr, int n_s
     if (j < n_tr && i < n_s) {
       const int jj = inv_perm[j];
       const float x0 = tile[threadIdx.x][r], x1 = tile[threadIdx.x + 1][r];
-      out[(int64_t)jj * S + i + 1] = make_float2(x0, x1 - x0);
-      if (i == 0) out[(int64_t)jj * S] = make_float2(0.f, x0);
+      out[(int64_t)jj * S + i + 1] = row_entry(x0, x1, i + 1, q0);
+      if (i == 0) out[(int64_t)jj * S] = row_entry(0.f, x0, 0, q0);
     }
   }
 }
 
 __global__ void stage_rows_x2_kernel(const float* tr, int64_t n_tr, int n_s, const int* perm,
-                                     int S, float2* out) {
+                                     int S, int q0, float2* out) {
   const int64_t jj = blockIdx.x;
   const float* x = tr + (int64_t)perm[jj] * n_s;
   for (int i = (int)threadIdx.x - 1; i < n_s; i += blockDim.x) {
     const float x0 = i >= 0 ? x[i] : 0.f;
     const float x1 = i + 1 < n_s ? x[i + 1] : 0.f;
-    out[jj * S + i + 1] = make_float2(x0, x1 - x0);
+    out[jj * S + i + 1] = row_entry(x0, x1, i + 1, q0);
   }
 }
 
@@ -650,6 +655,8 @@ static pstm_status validate(const pstm_grid* g, const pstm_params* prm, const ps
     return fail(PSTM_EINVAL, "aa_max_halfwidth must be in [1, 256] samples");
   if (prm->antialias && (!(prm->aa_dx >= 0) || !(prm->aa_dy >= 0)))
     return fail(PSTM_EINVAL, "aa_dx/aa_dy must be non-negative");
+  if (prm->forward_only != 0 && prm->forward_only != 1)
+    return fail(PSTM_EINVAL, "forward_only must be 0 or 1");
   if (prm->antialias && prm->weight != PSTM_WEIGHT_OBLIQUITY_SPREADING)
     return fail(PSTM_ENOTSUP, "the anti-alias kernel is built for the obliquity x spreading weight");
   if (geo->n_traces < 0 || geo->n_traces > (int64_t)INT32_MAX)
@@ -719,6 +726,8 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
     // (x[i], x[i+1] - x[i]) entries for i = -1 .. N-1 at row positions i + 1
     p->row_stride = (int)align_up(prm->n_samples + 1, 8);
     p->elt_bytes = 8;
+    // migration-only plans: intercept form about the middle entry
+    if (prm->forward_only) p->row_origin = (prm->n_samples + 1) / 2;
   }
   if (prm->antialias) {
     // rows hold the trend-removed double integral I2[-pad .. N + pad] in float32
@@ -961,10 +970,10 @@ pstm_status pstm_load_traces(pstm_plan* plan, const float* traces, int32_t trace
   if (p->params.storage == PSTM_F32) {
     if (trace_major)
       stage_rows_x2_kernel<<<(unsigned)n, 256, 0, s>>>(traces, n, n_s, p->perm, p->row_stride,
-                                                       (float2*)p->traces);
+                                                       p->row_origin, (float2*)p->traces);
     else
       stage_transpose_x2_kernel<<<tg, tb, 0, s>>>(traces, n, n_s, p->inv_perm, p->row_stride,
-                                                  (float2*)p->traces);
+                                                  p->row_origin, (float2*)p->traces);
   } else if (p->params.storage == PSTM_BF16) {
     PSTM_STAGE(__nv_bfloat16)
   } else {
@@ -1057,6 +1066,8 @@ pstm_status pstm_velocity_gradient(pstm_plan* plan, const float* grad_image, con
   if (p->params.weight != PSTM_WEIGHT_OBLIQUITY_SPREADING || p->params.antialias)
     return fail(PSTM_ENOTSUP, "velocity gradient is built for the plain obliquity x spreading "
                               "operator");
+  if (p->params.forward_only && p->params.storage == PSTM_F32)
+    return fail(PSTM_ENOTSUP, "velocity gradient needs a plan built without forward_only");
   pstm_status st = check_velocity_args(vel, vst, vsc);
   if (st != PSTM_OK) return st;
   std::string why;

@@ -158,7 +158,7 @@ class MigrationEngine:
                             storage=self.storage, variant=self.variant,
                             kernel_backend=kernel_backend or self.kernel_backend,
                             antialias=antialias, aa_dx=il_spacing, aa_dy=xl_spacing,
-                            aa_max_halfwidth=aa_max_halfwidth)
+                            aa_max_halfwidth=aa_max_halfwidth, forward_only=True)
             try:
                 if progress_callback:
                     progress_callback(0.1, "Running Kirchhoff migration...")

@@ -66,7 +66,11 @@ class PSTMPlan:
 
     Coordinates may be float32 or float64 (world, e.g. UTM); the grid origin is
     subtracted in float64 on the device and everything downstream is grid-local
-    float32.
+    float32.  ``forward_only=True`` is for plans that only migrate: float32
+    traces are staged in intercept form (one FMA per interpolation tap, ~3 %
+    faster); ``demigrate`` then matches the migration's transpose to ~1e-5
+    rather than to float rounding, and ``velocity_gradient`` and batches refuse
+    the plan.
     """
 
     def __init__(self, source_x, source_y, receiver_x, receiver_y, *, n_il: int, n_xl: int,
@@ -76,7 +80,8 @@ class PSTMPlan:
                  time_dependent_aperture: bool = False, weight: str = "obliquity_spreading",
                  clamp: str = "full", storage: str = "f32", variant: int = 0,
                  kernel_backend=None, antialias: bool = False, aa_dx: float = 0.0,
-                 aa_dy: float = 0.0, aa_max_halfwidth: float = 32.0):
+                 aa_dy: float = 0.0, aa_max_halfwidth: float = 32.0,
+                 forward_only: bool = False):
         require_cuda(kernel_backend)
         self._lib = _lib.lib()
         self._handle = C.c_void_p(None)
@@ -104,7 +109,7 @@ class PSTMPlan:
                                   int(bool(time_dependent_aperture)), WEIGHTS[weight],
                                   CLAMPS[clamp], STORAGES[storage], int(bool(antialias)),
                                   float(aa_dx), float(aa_dy), float(aa_max_halfwidth),
-                                  int(variant))
+                                  int(variant), int(bool(forward_only)))
         geo = _lib.Geometry(n_tr, _lib.PSTM_F64 if dt == torch.float64 else _lib.PSTM_F32,
                             *[c.data_ptr() for c in coords])
         _lib.check(self._lib.pstm_plan_create(C.byref(self._handle), C.byref(self.grid),
@@ -322,7 +327,7 @@ def migrate_kirchhoff_full(traces: torch.Tensor, source_x: torch.Tensor, source_
                     t0_ms=t0, dt_ms=dto, n_samples=n_s, in_t0_ms=t_min_ms, in_dt_ms=dt_ms,
                     max_aperture_m=max_aperture_m, max_angle_deg=max_angle_deg,
                     time_dependent_aperture=use_time_dependent_aperture, storage=storage,
-                    variant=variant, kernel_backend=kernel_backend)
+                    variant=variant, kernel_backend=kernel_backend, forward_only=True)
     try:
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)] if enable_profiling else None
         if ev:

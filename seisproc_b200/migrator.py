@@ -238,7 +238,7 @@ class KirchhoffMigrator(BaseMigrator):
                 weight=_WEIGHT_OF_MODE[self.config.weight_mode], clamp="migrator",
                 storage=self.storage, variant=self.variant, kernel_backend=self.kernel_backend,
                 antialias=self.antialias, aa_dx=g.d_inline, aa_dy=g.d_xline,
-                aa_max_halfwidth=self.aa_max_halfwidth)
+                aa_max_halfwidth=self.aa_max_halfwidth, forward_only=True)
             try:
                 v = self._velocity_grid()
                 tr = torch.from_numpy(np.ascontiguousarray(traces, dtype=np.float32))

@@ -50,6 +50,11 @@ def test_plan_create_rejects_bad_config_without_device():
                               None) == _lib.PSTM_EINVAL
     assert "max_angle_deg" in _lib.last_error()
     params.max_angle_deg = 60.0
+    params.forward_only = 2
+    assert L.pstm_plan_create(C.byref(h), C.byref(grid), C.byref(params), C.byref(geo),
+                              None) == _lib.PSTM_EINVAL
+    assert "forward_only" in _lib.last_error()
+    params.forward_only = 0
     params.storage = 9
     assert L.pstm_plan_create(C.byref(h), C.byref(grid), C.byref(params), C.byref(geo),
                               None) == _lib.PSTM_EINVAL

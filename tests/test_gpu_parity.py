@@ -223,6 +223,55 @@ def test_output_before_first_input_sample():
     assert np.abs(fold - of).sum() <= max(2, FOLD_FLIP_FRAC * of.sum())
 
 
+@pytest.mark.parametrize("weight", ["obliquity_spreading", "spreading", "obliquity", "none"])
+def test_forward_only_rows_match_fp64_oracle(weight):
+    """Plans built forward_only stage intercept-form float32 rows: the same
+    operator to float rounding (vs the default plan and vs FP64)."""
+    s = _small_3d(seed=6)
+    img, fold = _plan_3d(s, weight=weight, forward_only=True)
+    ref, rfold = _plan_3d(s, weight=weight)
+    oi, of = _oracle_3d(s, weight=weight)
+    assert rel_l2(img, oi) <= FP32_TOL, weight
+    assert rel_l2(img, ref) <= 1e-5, weight
+    assert np.array_equal(fold, rfold)
+
+
+def test_forward_only_low_clamp_and_16bit():
+    """The intercept frame under the low clamp (traces starting 40 ms late), and
+    forward_only leaving 16-bit rows untouched."""
+    s = _small_3d(seed=7)
+    img, fold = _plan_3d(s, in_t0_ms=40.0, forward_only=True)
+    ref, rfold = _plan_3d(s, in_t0_ms=40.0)
+    assert rel_l2(img, ref) <= 1e-5 and np.array_equal(fold, rfold)
+    b1, _ = _plan_3d(s, storage="bf16", forward_only=True)
+    b0, _ = _plan_3d(s, storage="bf16")
+    assert np.array_equal(b1, b0)
+
+
+def test_forward_only_plan_refuses_gradient_and_batch():
+    from seisproc_b200.batched import BatchedPSTM
+    from seisproc_b200.kirchhoff import PSTMPlan
+    s = _small_3d(seed=8, n_traces=1000)
+    dev = torch.device("cuda")
+    c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    plan = PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+                    origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                    xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                    in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                    max_angle_deg=s.max_angle_deg, forward_only=True)
+    v = torch.from_numpy(s.vrms).to(dev)
+    img, _ = plan.migrate(s.traces.to(dev), v)
+    with pytest.raises(Exception, match="forward_only"):
+        plan.velocity_gradient(img, v)
+    with pytest.raises(Exception, match="forward_only"):
+        BatchedPSTM([plan], v)
+    d = plan.demigrate(img, v)  # still the adjoint, to ~1e-5
+    assert d.shape == s.traces.shape
+    plan.check()
+    plan.close()
+
+
 def test_plans_reuse_pooled_memory_and_trim():
     """Plans built and destroyed one after another take their memory from the
     library's pool; results stay the same, and trimming returns it."""
