@@ -179,8 +179,10 @@ def survey_2d(seed: int = 1234, device="cpu", n_offsets: int = 12, n_cmp: int = 
 
 def vrms_3d(t0_s: np.ndarray, x: np.ndarray, y: np.ndarray, t_max_s: float,
             extent: float = 5000.0) -> np.ndarray:
-    """V_rms(t0, x, y) = (1500 + 2000 t0/t_max) (1 + 0.05 sin(2 pi x/L) sin(2 pi y/L))."""
-    return (1500.0 + 2000.0 * t0_s / t_max_s) * (
+    """V_rms(t0, x, y) = (1500 + 2000 t0/t_max) (1 + 0.05 sin(2 pi x/L) sin(2 pi y/L));
+    a single output time (t_max = 0) takes the 1500 m/s trend value."""
+    ramp = 2000.0 * t0_s / t_max_s if t_max_s > 0 else 0.0 * t0_s
+    return (1500.0 + ramp) * (
         1.0 + 0.05 * np.sin(2 * np.pi * x / extent) * np.sin(2 * np.pi * y / extent))
 
 
