@@ -423,6 +423,8 @@ def bench_ours(args):
                 fold_cols = float(fold_cols_t[:, torch.from_numpy(cols).to(dev)].double().sum())
                 cb = run_cpu_port(s, cols, fold_cols)
                 cb.pop("seconds", None)
+                # the whole workload at the crop's rate (extrapolated, not run)
+                cb["full_workload_s_extrapolated"] = pairs_all / (cb["value"] * 1e9)
         result = {
             "metric": "PSTM Gpairs/s (out-sample x trace)", "value": value, "unit": "Gpairs/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
