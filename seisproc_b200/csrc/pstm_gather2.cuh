@@ -242,12 +242,13 @@ __device__ __forceinline__ void sweep_aa(f2 (&acc)[M], const f2 (&zz)[M], const 
     }
 #pragma unroll
     for (int n = 0; n < NTR; ++n) {
-      const f2 rrs = f2_add(f2_bcast(hs2[n]), zz[i]);
-      const f2 rrr = f2_add(f2_bcast(hr2[n]), zz[i]);
+      // pre-scaled as the plain sweep: zz = a^2 (z^2 + eps), aa = a^2, q' = q / a;
+      // g' = g / a, so L = a max(|g_x|, |g_y|) = aa max(|g'_x|, |g'_y|)
+      const f2 rrs = f2_fma(f2_bcast(hs2[n]), aa[i], zz[i]);
+      const f2 rrr = f2_fma(f2_bcast(hr2[n]), aa[i], zz[i]);
       const f2 qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
       const f2 qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
-      const f2 sum = f2_fma(rrr, qr, f2_mul(rrs, qs));
-      f2 id = f2_fma(sum, aa[i], bb);
+      f2 id = f2_fma(rrr, qr, f2_fma(rrs, qs, bb));
       id.x = fminf(id.x, hi_c);
       id.y = fminf(id.y, hi_c);
       if constexpr (LOWC) {
@@ -372,7 +373,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     const float zh = depth_of(vh, out_time_ms(kh, A.out_dt, A.out_t0));
     zz[i] = f2{fmaf(zl, zl, kRadicandFloor), fmaf(zh, zh, kRadicandFloor)};
     aa[i] = f2{1000.0f / (vl * A.in_dt), 1000.0f / (vh * A.in_dt)};
-    if constexpr (!AA && kPrescaled<OP, WM>) {
+    if constexpr (kPrescaled<OP, WM>) {
       aa[i] = f2_mul(aa[i], aa[i]);
       zz[i] = f2_mul(zz[i], aa[i]);
     }
@@ -574,7 +575,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
       const float zh = depth_of(vh, out_time_ms(kh, A.out_dt, A.out_t0));
       fl = zl * zl;
       fh = zh * zh;
-      if constexpr (!AA && kPrescaled<OP, WM>) {
+      if constexpr (kPrescaled<OP, WM>) {
         // the pre-scaled weight p' = p / a^2: multiply by a^4 (p^2) or a^2 (p)
         const float al = 1000.0f / (vl * A.in_dt), ah = 1000.0f / (vh * A.in_dt);
         const float al2 = al * al, ah2 = ah * ah;
