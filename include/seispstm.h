@@ -103,6 +103,14 @@ typedef struct pstm_params {
                                   and pstm_velocity_gradient / batches reject the plan.
                                   0: (x, dx) rows, migration and demigration an exact float
                                   transpose pair (dot-product tests, least squares). */
+  double taper_width;          /* 0: hard masks only (what the reference migrators apply).
+                                  In (0, 1): also the aperture controller's cosine tapers
+                                  (processors/migration/aperture.py:228-270) of both legs:
+                                  distance from A (1 - w) to A, angle atan2(h, |z|) from
+                                  theta (1 - w) to theta.  Float32 storage, migration only
+                                  (demigration, V-gradient, batches and the anti-alias
+                                  filter refuse it); the fold still counts hard-masked
+                                  pairs.  The offset taper is per trace: scale the traces. */
 } pstm_params;
 
 typedef struct pstm_geometry {

@@ -92,6 +92,54 @@ def _column_terms(xc, yc, sx, sy, rx, ry, z, v, t_out_ms, n_s, in_dt_ms, in_t0_m
     return mask, rs, rr, hs, hr, idx, w, t_ms
 
 
+def _cosine_edge(x, start, end):
+    """1 up to ``start``, 0.5 (1 + cos(pi (x - start) / (end - start))) up to
+    ``end``, 0 beyond (processors/migration/aperture.py:228-270)."""
+    x = np.asarray(x, np.float64)
+    out = np.ones_like(x)
+    if end > start:
+        zone = (x > start) & (x <= end)
+        out = np.where(zone, 0.5 * (1.0 + np.cos(np.pi * (x - start) / (end - start))), out)
+    return np.where(x > end, 0.0, out)
+
+
+def distance_taper_fp64(h, max_distance, taper_width):
+    """ApertureController._compute_distance_taper (aperture.py:228-249)."""
+    return _cosine_edge(h, max_distance * (1.0 - taper_width), max_distance)
+
+
+def angle_taper_fp64(angle_rad, max_angle_rad, taper_width):
+    """ApertureController._compute_angle_taper (aperture.py:251-270)."""
+    return _cosine_edge(angle_rad, max_angle_rad * (1.0 - taper_width), max_angle_rad)
+
+
+def offset_taper_fp64(offset, min_offset, max_offset, taper_width):
+    """ApertureController._compute_offset_mask (aperture.py:197-226): 0 outside
+    [min, max], cosine rise over the first taper_width of the range and fall
+    over the last."""
+    o = np.asarray(offset, np.float64)
+    rng = taper_width * (max_offset - min_offset)
+    near = np.ones_like(o)
+    far = np.ones_like(o)
+    if rng > 0:
+        zn = (o >= min_offset) & (o < min_offset + rng)
+        near = np.where(zn, 0.5 * (1.0 - np.cos(np.pi * (o - min_offset) / rng)), 1.0)
+        zf = (o > max_offset - rng) & (o <= max_offset)
+        far = np.where(zf, 0.5 * (1.0 + np.cos(np.pi * (o - (max_offset - rng)) / rng)), 1.0)
+    return np.where((o >= min_offset) & (o <= max_offset), near * far, 0.0)
+
+
+def aperture_taper_fp64(hs, hr, z, aperture, angle_rad, taper_width):
+    """Distance and angle tapers of both legs, angle = atan2(h, |z|)
+    (ApertureController.compute_aperture_mask, aperture.py:65-147, without its
+    offset factor).  hs, hr: (n_tr, 1); z: (1, n_t)."""
+    az = np.abs(z)
+    return (distance_taper_fp64(hs, aperture, taper_width) *
+            distance_taper_fp64(hr, aperture, taper_width) *
+            angle_taper_fp64(np.arctan2(hs, az), angle_rad, taper_width) *
+            angle_taper_fp64(np.arctan2(hr, az), angle_rad, taper_width))
+
+
 def _candidates(xc, yc, sx, sy, rx, ry, aperture):
     """Traces whose legs are both inside the (largest) aperture of a column."""
     hs = np.hypot(xc - sx, yc - sy)
@@ -149,7 +197,7 @@ def triangle_explicit(tr: np.ndarray, i: int, L: int) -> float:
 def migrate_fp64(traces, sx, sy, rx, ry, out_x, out_y, t_out_ms, velocity, in_dt_ms,
                  in_t0_ms, aperture, angle_deg, time_dependent=False,
                  weight="obliquity_spreading", clamp="full", antialias=False, dx_out=0.0,
-                 dy_out=0.0, l_max=32.0, columns=None):
+                 dy_out=0.0, l_max=32.0, columns=None, taper_width=0.0):
     """Forward migration (data -> image) in float64.
 
     traces: (N_s, N_tr); coordinates float64 (any common origin);
@@ -157,7 +205,9 @@ def migrate_fp64(traces, sx, sy, rx, ry, out_x, out_y, t_out_ms, velocity, in_dt
     velocity: scalar, (N_t,) or (N_t, n_c) V_rms at the output samples.
     Returns image (N_t, n_c) and fold (N_t, n_c) as float64.
     ``columns`` optionally restricts the computation to a subset of columns
-    (others stay 0).
+    (others stay 0).  ``taper_width`` > 0 multiplies every weight by the
+    aperture controller's distance and angle cosine tapers of both legs
+    (``aperture_taper_fp64``); the fold still counts the hard-masked pairs.
     """
     tr = np.asarray(traces, dtype=np.float64)
     n_s, n_tr = tr.shape
@@ -187,6 +237,8 @@ def migrate_fp64(traces, sx, sy, rx, ry, out_x, out_y, t_out_ms, velocity, in_dt
         mask, rs, rr, hs, hr, idx, w, _ = _column_terms(
             out_x[c], out_y[c], sx[cand], sy[cand], rx[cand], ry[cand], z, v, t_out_ms, n_s,
             in_dt_ms, in_t0_ms, aperture, ang, time_dependent, weight, clamp)
+        if taper_width > 0:
+            w = w * aperture_taper_fp64(hs, hr, z[None, :], aperture, ang, taper_width)
         keep = np.nonzero(mask.any(axis=1))[0]
         if keep.size == 0:
             continue

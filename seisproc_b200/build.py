@@ -23,6 +23,7 @@ SOURCES = [
     "pstm_migrate.cu",
     "pstm_gather_fwd.cu",
     "pstm_gather_fwd_icpt.cu",
+    "pstm_gather_fwd_taper.cu",
     "pstm_adjoint.cu",
     "pstm_gather_vgrad.cu",
     "pstm_noalloc.cu",

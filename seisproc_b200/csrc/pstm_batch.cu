@@ -148,6 +148,11 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
       free_batch(b);
       return bfail(PSTM_ENOTSUP, "the batched launch is built for the plain operator");
     }
+    if (p->params.taper_width > 0) {
+      free_batch(b);
+      return bfail(PSTM_ENOTSUP, "the batched launch applies no aperture taper: build the "
+                                 "class plans without taper_width");
+    }
     if (p->params.forward_only && p->params.storage == PSTM_F32) {
       free_batch(b);
       return bfail(PSTM_ENOTSUP, "the batched launch reads (x, dx) float32 rows: build the "

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <string>
 #include <type_traits>
 
@@ -10,6 +11,15 @@
 #include "pstm_internal.h"
 
 namespace pstm {
+
+// The aperture controller's cosine tapers (opt-in; the reference migrators
+// construct the controller and never apply it): distance taper from d0 to the
+// aperture dmax, angle taper from a0 to the maximum angle amax (radians), both
+// legs; tan2 = tan^2(a0).  processors/migration/aperture.py:228-270.
+struct TaperArgs {
+  float d0, dinv, dmax;
+  float a0, ainv, amax, tan2;
+};
 
 struct KArgs {
   const float4* geo;
@@ -38,6 +48,7 @@ struct KArgs {
   float aa_dx, aa_dy, aa_lmax;
   int aa_pad;
   int row_origin;  // expanded rows: intercept origin (entry index)
+  TaperArgs tp;    // plans built with a taper width
 };
 
 __device__ __forceinline__ float vel_at(const KArgs& A, int k, int c) {
@@ -108,6 +119,34 @@ constexpr float kMagic = 8388608.0f;  // 2^23
 constexpr uint32_t kMagicBits = 0x4B000000u;
 constexpr float kRadicandFloor = 1e-12f;  // keeps rsqrt finite at r = 0 (m^2)
 
+// 1 up to start, 0.5 (1 + cos(pi (x - start) / (end - start))) up to end, 0
+// beyond (inv = 1 / (end - start)): the aperture controller's cosine edge.
+__device__ __forceinline__ float cos_edge(float x, float start, float inv, float end) {
+  if (x <= start) return 1.0f;
+  if (x > end) return 0.0f;
+  return 0.5f * (1.0f + cospif((x - start) * inv));
+}
+
+// Angle taper of one leg at one output sample, angle = atan2(h, |z|); z^2 comes
+// from the lane's constants (pre-scaled: zz = a^2 (z^2 + f), aa = a^2; else
+// zz = z^2 + f).  Below the taper start (h^2 <= z^2 tan^2(a0)) it is 1 without
+// the arctangent.
+// The taper zone proper, called rather than inlined: the unrolled sweeps
+// would otherwise carry dozens of copies of the arctangent and cosine.
+__device__ __noinline__ float angle_taper_zone(float h2, float z2, float a0, float ainv,
+                                               float amax) {
+  return cos_edge(atan2f(sqrtf(h2), sqrtf(fmaxf(z2, 0.0f))), a0, ainv, amax);
+}
+
+template <bool PRE>
+__device__ __forceinline__ float leg_angle_taper(float h2, float zz, float aa,
+                                                 const TaperArgs& tp) {
+  const float z2s = PRE ? fmaf(-aa, kRadicandFloor, zz) : zz - kRadicandFloor;
+  const float h2s = PRE ? h2 * aa : h2;
+  if (h2s <= z2s * tp.tan2) return 1.0f;
+  return angle_taper_zone(h2, PRE ? z2s / aa : z2s, tp.a0, tp.ainv, tp.amax);
+}
+
 inline KArgs make_args(const Plan* p, const float* vel, int64_t vst, int64_t vsc) {
   KArgs A;
   A.geo = p->geo;
@@ -150,6 +189,18 @@ inline KArgs make_args(const Plan* p, const float* vel, int64_t vst, int64_t vsc
   A.aa_lmax = (float)p->params.aa_max_halfwidth;
   A.aa_pad = p->aa_pad;
   A.row_origin = p->row_origin;
+  {
+    const double tw = p->params.taper_width;
+    const double ap = p->params.max_aperture_m, th = p->params.max_angle_deg * M_PI / 180.0;
+    const double d0 = ap * (1.0 - tw), a0 = th * (1.0 - tw);
+    A.tp.d0 = (float)d0;
+    A.tp.dinv = tw > 0 ? (float)(1.0 / (ap - d0)) : 0.0f;
+    A.tp.dmax = (float)ap;
+    A.tp.a0 = (float)a0;
+    A.tp.ainv = tw > 0 ? (float)(1.0 / (th - a0)) : 0.0f;
+    A.tp.amax = (float)th;
+    A.tp.tan2 = (float)(std::tan(a0) * std::tan(a0));
+  }
   return A;
 }
 

@@ -100,12 +100,13 @@ __device__ __forceinline__ float lds_elem<__half>(uint32_t addr) {
 // MASKED) and, for f16 storage, its scale.  A MASKED sweep starts at group g0,
 // the first 64-sample group holding a contributing sample of any of its traces
 // (warp-uniform, so the skipped groups cost one uniform branch each).
-template <int M, typename ST, int WM, bool LOWC, bool MASKED, int OP, int NTR>
+template <int M, typename ST, int WM, bool LOWC, bool MASKED, int OP, int NTR, bool TAPER>
 __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], const f2 (&aa)[M],
                                              const float (&hs2)[NTR], const float (&hr2)[NTR],
                                              const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
                                              const float (&sc)[NTR], f2 bb, f2 magic2,
-                                             float hi_c, float lo_c, int kw, int lane, int g0) {
+                                             float hi_c, float lo_c, int kw, int lane, int g0,
+                                             const TaperArgs& tp) {
   constexpr int ES = (int)sizeof(ST);
   constexpr int SHIFT = ES == 8 ? 3 : (ES == 4 ? 2 : 1);
 #pragma unroll
@@ -169,7 +170,14 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
         f2 w = p;
         if constexpr (WM == W_OBL_SPREAD) w = f2_mul(p, p);
         if constexpr (WM == W_NONE) w = f2_bcast(1.0f);
-        if constexpr (std::is_same<ST, __half>::value) w = f2_mul(w, f2_bcast(sc[n]));
+        // per-trace factor: f16 scale, or the distance tapers of both legs
+        if constexpr (std::is_same<ST, __half>::value || TAPER) w = f2_mul(w, f2_bcast(sc[n]));
+        if constexpr (TAPER) {
+          w.x *= leg_angle_taper<true>(hs2[n], zz[i].x, aa[i].x, tp) *
+                 leg_angle_taper<true>(hr2[n], zz[i].x, aa[i].x, tp);
+          w.y *= leg_angle_taper<true>(hs2[n], zz[i].y, aa[i].y, tp) *
+                 leg_angle_taper<true>(hr2[n], zz[i].y, aa[i].y, tp);
+        }
         if constexpr (MASKED) {
           const int klo = kw + 64 * i + lane;
           w.x = klo >= kst[n] ? w.x : 0.f;
@@ -188,7 +196,13 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
       } else {
         w = f2{1.0f, 1.0f};
       }
-      if constexpr (std::is_same<ST, __half>::value) w = f2_mul(w, f2_bcast(sc[n]));
+      if constexpr (std::is_same<ST, __half>::value || TAPER) w = f2_mul(w, f2_bcast(sc[n]));
+      if constexpr (TAPER) {
+        w.x *= leg_angle_taper<false>(hs2[n], zz[i].x, aa[i].x, tp) *
+               leg_angle_taper<false>(hr2[n], zz[i].x, aa[i].x, tp);
+        w.y *= leg_angle_taper<false>(hs2[n], zz[i].y, aa[i].y, tp) *
+               leg_angle_taper<false>(hr2[n], zz[i].y, aa[i].y, tp);
+      }
       if constexpr (MASKED) {
         const int klo = kw + 64 * i + lane;
         w.x = klo >= kst[n] ? w.x : 0.f;
@@ -277,7 +291,8 @@ __device__ __forceinline__ void sweep_aa(f2 (&acc)[M], const f2 (&zz)[M], const 
   }
 }
 
-template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP, bool AA = false>
+template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP, bool AA = false,
+          bool TAPER = false>
 __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, const int win,
                                             unsigned char* smem) {
   constexpr int NW = COLS * WPC;
@@ -432,6 +447,12 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         }
       }
       if (A.scales) tsc = __ldg(A.scales + jj);
+      if constexpr (TAPER) {
+        // the distance tapers of both legs: one factor per (column, trace)
+        if (warp_live)
+          tsc *= cos_edge(sqrtf(hs2), A.tp.d0, A.tp.dinv, A.tp.dmax) *
+                 cos_edge(sqrtf(hr2), A.tp.d0, A.tp.dinv, A.tp.dmax);
+      }
     }
     const int pn = p0 + 32 + lane;
     if (pn < n_list) jj_next = A.list[off0 + pn];
@@ -486,11 +507,12 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const uint32_t rb[2] = {rb0, rb0 + (uint32_t)RP};
         const int kk[2] = {ka, kb};
         if (ka > kw || kb > kw)
-          sweep_traces<M, ST, WM, LOWC, true, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c,
-                                                      lo_c, kw, lane, (min(ka, kb) - kw) >> 6);
+          sweep_traces<M, ST, WM, LOWC, true, OP, 2, TAPER>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
+                                                             hi_c, lo_c, kw, lane,
+                                                             (min(ka, kb) - kw) >> 6, A.tp);
         else
-          sweep_traces<M, ST, WM, LOWC, false, OP, 2>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c,
-                                                       lo_c, kw, lane, 0);
+          sweep_traces<M, ST, WM, LOWC, false, OP, 2, TAPER>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
+                                                              hi_c, lo_c, kw, lane, 0, A.tp);
       } else if (la || lb) {
         const int u = la ? t : t + 1;
         const float hs[1] = {__shfl_sync(0xffffffffu, hs2, u)};
@@ -499,11 +521,12 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const uint32_t rb[1] = {la ? rb0 : rb0 + (uint32_t)RP};
         const int kk[1] = {la ? ka : kb};
         if (kk[0] > kw)
-          sweep_traces<M, ST, WM, LOWC, true, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c,
-                                                      lo_c, kw, lane, (kk[0] - kw) >> 6);
+          sweep_traces<M, ST, WM, LOWC, true, OP, 1, TAPER>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
+                                                             hi_c, lo_c, kw, lane, (kk[0] - kw) >> 6,
+                                                             A.tp);
         else
-          sweep_traces<M, ST, WM, LOWC, false, OP, 1>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c,
-                                                       lo_c, kw, lane, 0);
+          sweep_traces<M, ST, WM, LOWC, false, OP, 1, TAPER>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
+                                                              hi_c, lo_c, kw, lane, 0, A.tp);
       }
       const int adv = pair ? 2 : 1;
       t += adv;
@@ -592,10 +615,11 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   }
 }
 
-template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP, bool AA = false>
+template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP, bool AA = false,
+          bool TAPER = false>
 __global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const KArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
-  gather_tile<COLS, WPC, M, ST, WM, LOWC, OP, AA>(A, blockIdx.x, blockIdx.y, smem);
+  gather_tile<COLS, WPC, M, ST, WM, LOWC, OP, AA, TAPER>(A, blockIdx.x, blockIdx.y, smem);
 }
 
 // Persistent batched kernel: CTAs pull (class, tile, window) work items from a
@@ -628,10 +652,11 @@ __global__ void __launch_bounds__(COLS* WPC * 32, 1)
   }
 }
 
-template <int COLS, int WPC, int M, typename ST, int WM, int OP, bool AA = false>
+template <int COLS, int WPC, int M, typename ST, int WM, int OP, bool AA = false,
+          bool TAPER = false>
 inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
-  auto kern = needs_lowclamp(p) ? pstm_gather2_kernel<COLS, WPC, M, ST, WM, true, OP, AA>
-                                : pstm_gather2_kernel<COLS, WPC, M, ST, WM, false, OP, AA>;
+  auto kern = needs_lowclamp(p) ? pstm_gather2_kernel<COLS, WPC, M, ST, WM, true, OP, AA, TAPER>
+                                : pstm_gather2_kernel<COLS, WPC, M, ST, WM, false, OP, AA, TAPER>;
   const int T = WPC * 64 * M;
   KArgs A2 = A;
   if (!ring_shape(COLS, T, p->row_stride, (int)sizeof(ST), &A2.ring_stages, &A2.ring_rows))
@@ -646,24 +671,24 @@ inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int COLS, int WPC, int M, typename ST, int OP>
+template <int COLS, int WPC, int M, typename ST, int OP, bool TAPER = false>
 inline cudaError_t dispatch2_wm(const Plan* p, const KArgs& A, cudaStream_t s) {
   const int wm = p->params.weight;
   constexpr bool k32 = std::is_same<ST, float>::value || std::is_same<ST, float2>::value ||
                       std::is_same<ST, RowIcpt>::value;
   if constexpr (OP == OP_VGRAD || !k32) {
     if (wm != W_OBL_SPREAD) return cudaErrorNotSupported;
-    return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP>(p, A, s);
+    return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP, false, TAPER>(p, A, s);
   } else {
     switch (wm) {
       case W_OBL_SPREAD:
-        return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP>(p, A, s);
+        return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP, false, TAPER>(p, A, s);
       case W_SPREAD:
-        return launch2_one<COLS, WPC, M, ST, W_SPREAD, OP>(p, A, s);
+        return launch2_one<COLS, WPC, M, ST, W_SPREAD, OP, false, TAPER>(p, A, s);
       case W_OBL:
-        return launch2_one<COLS, WPC, M, ST, W_OBL, OP>(p, A, s);
+        return launch2_one<COLS, WPC, M, ST, W_OBL, OP, false, TAPER>(p, A, s);
       case W_NONE:
-        return launch2_one<COLS, WPC, M, ST, W_NONE, OP>(p, A, s);
+        return launch2_one<COLS, WPC, M, ST, W_NONE, OP, false, TAPER>(p, A, s);
     }
     return cudaErrorInvalidValue;
   }
@@ -672,6 +697,9 @@ inline cudaError_t dispatch2_wm(const Plan* p, const KArgs& A, cudaStream_t s) {
 // Forward launch over intercept-form float32 rows (forward_only plans),
 // instantiated in its own translation unit (pstm_gather_fwd_icpt.cu).
 cudaError_t launch_forward_icpt(const Plan* p, const KArgs& A, cudaStream_t s);
+// Forward launch with the aperture tapers (float32 plans with a taper width),
+// instantiated in pstm_gather_fwd_taper.cu.
+cudaError_t launch_forward_taper(const Plan* p, const KArgs& A, cudaStream_t s);
 
 template <int COLS, int WPC, int M, int OP>
 inline cudaError_t dispatch2_st(const Plan* p, const KArgs& A, cudaStream_t s) {
@@ -686,6 +714,12 @@ inline cudaError_t dispatch2_st(const Plan* p, const KArgs& A, cudaStream_t s) {
       // plans stage expanded (x, dx) rows, forward_only plans intercept-form
       // rows; the no-allocation path plain rows
       if (p->elt_bytes != 8) return dispatch2_wm<COLS, WPC, M, float, OP>(p, A, s);
+      if (p->params.taper_width > 0) {
+        if constexpr (OP == OP_FWD)
+          return launch_forward_taper(p, A, s);
+        else
+          return cudaErrorNotSupported;
+      }
       if (p->row_origin != 0) {
         if constexpr (OP == OP_FWD)
           return launch_forward_icpt(p, A, s);

@@ -657,6 +657,11 @@ static pstm_status validate(const pstm_grid* g, const pstm_params* prm, const ps
     return fail(PSTM_EINVAL, "aa_dx/aa_dy must be non-negative");
   if (prm->forward_only != 0 && prm->forward_only != 1)
     return fail(PSTM_EINVAL, "forward_only must be 0 or 1");
+  if (!(prm->taper_width >= 0.0 && prm->taper_width < 1.0))
+    return fail(PSTM_EINVAL, "taper_width must be in [0, 1)");
+  if (prm->taper_width > 0 && (prm->storage != PSTM_F32 || prm->antialias))
+    return fail(PSTM_ENOTSUP, "the aperture taper is built for float32 storage without the "
+                              "anti-alias filter");
   if (prm->antialias && prm->weight != PSTM_WEIGHT_OBLIQUITY_SPREADING)
     return fail(PSTM_ENOTSUP, "the anti-alias kernel is built for the obliquity x spreading weight");
   if (geo->n_traces < 0 || geo->n_traces > (int64_t)INT32_MAX)
@@ -738,6 +743,14 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
   }
   if (!shape_for_variant(prm->variant, g->n_xl, g->n_times, &p->shape))
     return fail(PSTM_EINVAL, "unknown kernel variant");
+  if (prm->taper_width > 0) {
+    // the tapered kernel is built for the 16-column shapes only
+    if (prm->variant == 0) {
+      shape_for_variant(g->n_xl < 2 ? 9 : 3, g->n_xl, g->n_times, &p->shape);
+    } else if (p->shape.id != 3 && p->shape.id != 9) {
+      return fail(PSTM_ENOTSUP, "the aperture taper runs kernel variants 3 and 9 only");
+    }
+  }
   p->tiles_il = (g->n_il + p->shape.tile_il - 1) / p->shape.tile_il;
   p->tiles_xl = (g->n_xl + p->shape.tile_xl - 1) / p->shape.tile_xl;
   p->n_tiles = (int64_t)p->tiles_il * p->tiles_xl;
@@ -1032,6 +1045,8 @@ pstm_status pstm_demigrate(pstm_plan* plan, const float* image, const float* vel
   Plan* p = reinterpret_cast<Plan*>(plan);
   if (p->params.antialias)
     return fail(PSTM_ENOTSUP, "demigration is built for the plain (non-anti-aliased) operator");
+  if (p->params.taper_width > 0)
+    return fail(PSTM_ENOTSUP, "demigration needs a plan built without taper_width");
   pstm_status st = check_velocity_args(vel, vst, vsc);
   if (st != PSTM_OK) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -1068,6 +1083,8 @@ pstm_status pstm_velocity_gradient(pstm_plan* plan, const float* grad_image, con
                               "operator");
   if (p->params.forward_only && p->params.storage == PSTM_F32)
     return fail(PSTM_ENOTSUP, "velocity gradient needs a plan built without forward_only");
+  if (p->params.taper_width > 0)
+    return fail(PSTM_ENOTSUP, "velocity gradient needs a plan built without taper_width");
   pstm_status st = check_velocity_args(vel, vst, vsc);
   if (st != PSTM_OK) return st;
   std::string why;

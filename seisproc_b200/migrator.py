@@ -159,13 +159,30 @@ class MigrationResult:
                 "fold_mean": float(np.mean(f)) if f is not None else None}
 
 
+def offset_taper(offset: np.ndarray, min_offset: float, max_offset: float,
+                 taper_width: float) -> np.ndarray:
+    """Per-trace weight of the aperture controller's offset mask
+    (processors/migration/aperture.py:197-226): 0 outside [min, max], a cosine
+    rise over the first ``taper_width`` of the range and a fall over the last."""
+    o = np.asarray(offset, np.float64)
+    span = taper_width * (max_offset - min_offset)
+    w = ((o >= min_offset) & (o <= max_offset)).astype(np.float64)
+    if span > 0:
+        rise = (o >= min_offset) & (o < min_offset + span)
+        w = np.where(rise, w * 0.5 * (1.0 - np.cos(np.pi * (o - min_offset) / span)), w)
+        fall = (o > max_offset - span) & (o <= max_offset)
+        w = np.where(fall, w * 0.5 * (1.0 + np.cos(np.pi * (o - max_offset + span) / span)), w)
+    return w
+
+
 class KirchhoffMigrator(BaseMigrator):
     """Output-driven Kirchhoff PSTM on the CUDA sm_100a kernels."""
 
     def __init__(self, velocity: VelocityModel, config: MigrationConfig,
                  device: Optional[torch.device] = None, use_traveltime_lut: bool = True,
                  kernel_backend=None, storage: str = "f32", variant: int = 0,
-                 antialias: bool = False, aa_max_halfwidth: float = 32.0):
+                 antialias: bool = False, aa_max_halfwidth: float = 32.0,
+                 aperture_taper: bool = False):
         self.velocity = velocity
         require_cuda(kernel_backend)
         self.device = torch.device(device) if device is not None else \
@@ -180,6 +197,9 @@ class KirchhoffMigrator(BaseMigrator):
         # explicit opt-in here (weight FULL only)
         self.antialias = antialias
         self.aa_max_halfwidth = aa_max_halfwidth
+        # likewise the aperture controller's cosine tapers (config.taper_width:
+        # offset per trace, distance and angle per leg), float32 storage only
+        self.aperture_taper = aperture_taper
         super().__init__(velocity, config)
 
     def _validate_inputs(self):
@@ -224,6 +244,10 @@ class KirchhoffMigrator(BaseMigrator):
             return output_image, output_fold
         full = sel.size == geometry.n_traces
         traces = gather.traces if full else gather.traces[:, sel]
+        tw = float(self.config.taper_width) if self.aperture_taper else 0.0
+        if tw > 0:
+            w_off = offset_taper(off[sel], self.config.min_offset_m, self.config.max_offset_m, tw)
+            traces = np.asarray(traces, np.float32) * w_off[None, :].astype(np.float32)
         coords = [a if full else a[sel] for a in (geometry.source_x, geometry.source_y,
                                                   geometry.receiver_x, geometry.receiver_y)]
         with torch.cuda.device(self.device):
@@ -238,7 +262,7 @@ class KirchhoffMigrator(BaseMigrator):
                 weight=_WEIGHT_OF_MODE[self.config.weight_mode], clamp="migrator",
                 storage=self.storage, variant=self.variant, kernel_backend=self.kernel_backend,
                 antialias=self.antialias, aa_dx=g.d_inline, aa_dy=g.d_xline,
-                aa_max_halfwidth=self.aa_max_halfwidth, forward_only=True)
+                aa_max_halfwidth=self.aa_max_halfwidth, forward_only=True, taper_width=tw)
             try:
                 v = self._velocity_grid()
                 tr = torch.from_numpy(np.ascontiguousarray(traces, dtype=np.float32))

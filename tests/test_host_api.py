@@ -127,3 +127,16 @@ def test_synthetic_noise_is_keyed_and_deterministic():
     assert torch.equal(s1.traces, s2.traces)
     c = synthetic.class_counts_loguniform()
     assert c.shape == (64,) and c.min() >= 2000 and c.max() <= 40000
+
+
+def test_offset_taper_matches_reference_controller():
+    """The migrator's per-trace offset taper against the reference's
+    ApertureController._compute_offset_mask (golden vectors)."""
+    import os
+    from conftest import ROOT
+    from seisproc_b200.migrator import offset_taper
+    g = np.load(os.path.join(ROOT, "tests", "golden", "aperture_taper.npz"))
+    off = np.hypot(g["rx"] - g["sx"], g["ry"] - g["sy"])
+    for k in range(2):
+        tw, _, _, omin, omax = g[f"params{k}"]
+        assert np.allclose(offset_taper(off, omin, omax, tw), g[f"offset_mask{k}"], atol=2e-6)

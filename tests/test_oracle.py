@@ -202,3 +202,26 @@ def test_oracle_vgrad_matches_finite_difference():
                                                    0.0, 1e5, 89.0)[0]))
     fd = (f(v + eps * dv) - f(v - eps * dv)) / (2 * eps)
     assert float(np.sum(gv * dv)) == pytest.approx(fd, rel=2e-3)
+
+
+def test_aperture_tapers_match_reference_controller():
+    """The FP64 restatement of ApertureController's offset, distance and angle
+    cosine tapers against the reference's own compute_aperture_mask."""
+    import os
+    from conftest import ROOT
+    g = np.load(os.path.join(ROOT, "tests", "golden", "aperture_taper.npz"))
+    sx, sy, rx, ry = g["sx"], g["sy"], g["rx"], g["ry"]
+    ix, iy, iz = g["ix"], g["iy"], g["iz"]
+    for k in range(2):
+        tw, a, th, omin, omax = g[f"params{k}"]
+        off = np.hypot(rx - sx, ry - sy)
+        om = O.offset_taper_fp64(off, omin, omax, tw)
+        assert np.allclose(om, g[f"offset_mask{k}"], atol=2e-6)
+        hs = np.hypot(ix[None, :] - sx[:, None], iy[None, :] - sy[:, None])  # (n_tr, n_xy)
+        hr = np.hypot(ix[None, :] - rx[:, None], iy[None, :] - ry[:, None])
+        want = g[f"mask{k}"]  # (n_z, n_tr, n_xy)
+        for q, z in enumerate(iz):
+            got = O.aperture_taper_fp64(hs, hr, np.full((1, 1), z), a, np.radians(th), tw)
+            got = got * om[:, None]
+            assert np.allclose(got, want[q], atol=2e-5), (k, q)
+        assert ((want > 0) & (want < 1)).any()  # the tapers are exercised
