@@ -372,6 +372,37 @@ def bench_ours(args):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e_ms, "ms_calls": [round(c, 1) for c in calls],
                "statistic": "median call"}
+        # the reference worker's calling pattern: a bin's traces come from a
+        # reader as (n_traces, n_samples) pageable arrays; streamed here through
+        # page-locked chunks into trace-major staging (no host transpose)
+        if world == 1:
+            from seisproc_b200.ingest import NumpyDataReader
+            reader = NumpyDataReader(np.ascontiguousarray(host_tr.numpy().T))
+            idx = np.arange(reader.n_traces)
+            c_np = [h.numpy() for h in host_c]
+            run_r = lambda: eng.migrate_bin_from_reader(reader, idx, *c_np,
+                                                        velocity_model=host_v.numpy(), **kw)
+            run_r()
+            rc = []
+            for _ in range(3):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                run_r()
+                rc.append((time.perf_counter() - t0) * 1e3)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.migrate_bin_full(reader.read_traces(idx).T, *c_np,
+                                 velocity_model=host_v.numpy(), **kw)
+            ref_ms = (time.perf_counter() - t0) * 1e3
+            r_ms = statistics.median(rc)
+            e2e["reader"] = {
+                "value": pairs_all / (r_ms * 1e-3) / 1e9, "unit": "Gpairs/s", "ms_per_step": r_ms,
+                "ms_calls": [round(c, 1) for c in rc],
+                "source": "NumpyDataReader over a pageable (n_traces, n_samples) array",
+                "reference_pattern_ms": ref_ms,
+                "reference_pattern": "read_traces(idx).T then migrate_bin_full (host transpose "
+                                     "and pageable upload), one call"}
+            del reader
 
     result = None
     if rank == 0:

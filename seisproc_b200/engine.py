@@ -109,12 +109,91 @@ class MigrationEngine:
         ``antialias`` applies the causal-integrated triangle filter whose
         half-width follows the operator dip times the bin spacing (capped at
         ``aa_max_halfwidth`` input samples)."""
-        t_start = time.perf_counter()
         require_cuda(kernel_backend if kernel_backend is not None else self.kernel_backend)
         traces = np.asarray(traces)
         if traces.ndim != 2:
             raise ValueError(f"traces must be (n_samples, n_traces), got {traces.shape}")
         n_s, n_tr = traces.shape
+
+        def upload(stream):
+            # the host array must outlive the asynchronous copy: it is returned
+            host_tr = np.ascontiguousarray(traces, dtype=np.float32)
+            with torch.cuda.stream(stream):
+                tr = torch.from_numpy(host_tr).to(self.device, non_blocking=True)
+            return (lambda: tr), False, host_tr
+
+        return self._migrate(upload, n_s, n_tr, source_x, source_y, receiver_x, receiver_y,
+                             origin_x, origin_y, il_spacing, xl_spacing, n_il, n_xl, dt_ms,
+                             t_min_ms, n_times, velocity_mps, max_aperture_m, max_angle_deg,
+                             normalize, min_fold, progress_callback, enable_profiling,
+                             use_time_dependent_aperture, velocity_model, kernel_backend,
+                             antialias, aa_max_halfwidth)
+
+    def migrate_bin_from_reader(
+        self,
+        reader,
+        trace_numbers: np.ndarray,
+        source_x: np.ndarray,
+        source_y: np.ndarray,
+        receiver_x: np.ndarray,
+        receiver_y: np.ndarray,
+        origin_x: float,
+        origin_y: float,
+        il_spacing: float,
+        xl_spacing: float,
+        azimuth_deg: float,
+        n_il: int,
+        n_xl: int,
+        dt_ms: float,
+        t_min_ms: float,
+        n_times: int = None,
+        velocity_mps: float = 2500.0,
+        max_aperture_m: float = 5000.0,
+        max_angle_deg: float = 60.0,
+        normalize: bool = True,
+        min_fold: int = 1,
+        progress_callback: Optional[Callable[[float, str], None]] = None,
+        enable_profiling: bool = False,
+        use_time_dependent_aperture: bool = False,
+        velocity_model=None,
+        kernel_backend=None,
+        antialias: bool = False,
+        aa_max_halfwidth: float = 32.0,
+        chunk_traces: int = 16384,
+        reader_threads: int = 8,
+    ) -> Tuple[np.ndarray, np.ndarray]:
+        """``migrate_bin_full`` with the traces ``trace_numbers`` taken from a
+        ``DataReader`` (``read_traces`` -> (n, n_samples); seisio/gather_readers.py:102-142)
+        instead of a transposed host array: they stream into device memory
+        through page-locked chunks while the plan is built, and are staged
+        from their trace-major layout.  Coordinates are those of the selected
+        traces, in the same order."""
+        from .ingest import TraceUpload
+        require_cuda(kernel_backend if kernel_backend is not None else self.kernel_backend)
+        idx = np.asarray(trace_numbers, np.int64)
+        n_s, n_tr = int(reader.get_n_samples()), int(idx.size)
+
+        def upload(stream):
+            up = TraceUpload(reader, idx, self.device, stream, chunk_traces=chunk_traces,
+                             threads=reader_threads)
+            return up.result, True, None
+
+        return self._migrate(upload, n_s, n_tr, source_x, source_y, receiver_x, receiver_y,
+                             origin_x, origin_y, il_spacing, xl_spacing, n_il, n_xl, dt_ms,
+                             t_min_ms, n_times, velocity_mps, max_aperture_m, max_angle_deg,
+                             normalize, min_fold, progress_callback, enable_profiling,
+                             use_time_dependent_aperture, velocity_model, kernel_backend,
+                             antialias, aa_max_halfwidth)
+
+    def _migrate(self, upload, n_s, n_tr, source_x, source_y, receiver_x, receiver_y, origin_x,
+                 origin_y, il_spacing, xl_spacing, n_il, n_xl, dt_ms, t_min_ms, n_times,
+                 velocity_mps, max_aperture_m, max_angle_deg, normalize, min_fold,
+                 progress_callback, enable_profiling, use_time_dependent_aperture,
+                 velocity_model, kernel_backend, antialias, aa_max_halfwidth):
+        """The body shared by the entry points.  ``upload(stream)`` starts the
+        traces' copy on ``stream`` and returns (wait() -> device tensor,
+        trace_major, host buffer to keep alive)."""
+        t_start = time.perf_counter()
         n_t = int(n_times) if n_times is not None else n_s
         if progress_callback:
             progress_callback(0.0, "Preparing data...")
@@ -122,14 +201,10 @@ class MigrationEngine:
             cur = torch.cuda.current_stream(self.device)
             # The traces (the bulk of the input) go up on a side stream while the
             # plan, which needs only the coordinates, is built on this one.
-            host_tr = np.ascontiguousarray(traces, dtype=np.float32)
             if self._copy_stream is None:
                 self._copy_stream = torch.cuda.Stream(self.device)
             self._copy_stream.wait_stream(cur)
-            with torch.cuda.stream(self._copy_stream):
-                tr = torch.from_numpy(host_tr).to(self.device, non_blocking=True)
-                tr_ready = torch.cuda.Event()
-                tr_ready.record(self._copy_stream)
+            tr_wait, trace_major, host_keep = upload(self._copy_stream)
             coords = []
             for a in (source_x, source_y, receiver_x, receiver_y):
                 a = np.asarray(a)
@@ -164,10 +239,11 @@ class MigrationEngine:
                     progress_callback(0.1, "Running Kirchhoff migration...")
                 ev0 = torch.cuda.Event(enable_timing=True)
                 ev1 = torch.cuda.Event(enable_timing=True)
-                cur.wait_event(tr_ready)
+                tr = tr_wait()
+                cur.wait_stream(self._copy_stream)
                 tr.record_stream(cur)
                 ev0.record()
-                image, fold = plan.migrate(tr, vel_t)
+                image, fold = plan.migrate(tr, vel_t, trace_major=trace_major)
                 ev1.record()
                 plan.check()
                 self.last_stats = dict(plan.stats())
