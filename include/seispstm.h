@@ -162,6 +162,16 @@ pstm_status pstm_plan_get_stats(const pstm_plan* plan, pstm_plan_stats* stats);
  * torch's allocator; torch.cuda.empty_cache is the analogue). */
 pstm_status pstm_trim_memory(int64_t keep_bytes);
 
+/* Copies traces first .. first + count - 1 of a host (n_samples, n_traces)
+ * float32 array (the reference's sample-major layout) into a device
+ * (n_samples, count) array, as one strided asynchronous copy on `stream` (the
+ * host array should be page-locked for the copy to be asynchronous).  It lets
+ * a caller upload a bin in blocks of traces and migrate each block (one plan
+ * per block) while the next one is in flight; no counterpart in the reference. */
+pstm_status pstm_copy_trace_columns(float* dst, const float* src, int64_t n_samples,
+                                   int64_t n_traces, int64_t first, int64_t count,
+                                   void* stream);
+
 /* Loads traces into the plan's spatially sorted, trace-major device copy in the
  * plan's storage dtype (per-trace float32 scale for BF16/F16; for the
  * anti-alias filter, the trend-removed double integral).  `traces` is

@@ -77,6 +77,8 @@ _SIGNATURES = {
     "pstm_plan_destroy": (C.c_int, [_P]),
     "pstm_plan_get_stats": (C.c_int, [_P, C.POINTER(PlanStats)]),
     "pstm_trim_memory": (C.c_int, [C.c_int64]),
+    "pstm_copy_trace_columns": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                                          _P]),
     "pstm_load_traces": (C.c_int, [_P, _P, C.c_int32, _P]),
     "pstm_migrate_loaded": (C.c_int, [_P, _P, C.c_int64, C.c_int64, _P, _P, _P]),
     "pstm_migrate": (C.c_int, [_P, _P, C.c_int32, _P, C.c_int64, C.c_int64, _P, _P, _P]),

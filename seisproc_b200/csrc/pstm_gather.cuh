@@ -133,8 +133,8 @@ __device__ __forceinline__ float cos_edge(float x, float start, float inv, float
 // the arctangent.
 // The taper zone proper, called rather than inlined: the unrolled sweeps
 // would otherwise carry dozens of copies of the arctangent and cosine.
-__device__ __noinline__ float angle_taper_zone(float h2, float z2, float a0, float ainv,
-                                               float amax) {
+static __device__ __noinline__ float angle_taper_zone(float h2, float z2, float a0, float ainv,
+                                                      float amax) {
   return cos_edge(atan2f(sqrtf(h2), sqrtf(fmaxf(z2, 0.0f))), a0, ainv, amax);
 }
 

@@ -904,6 +904,20 @@ pstm_status pstm_plan_destroy(pstm_plan* plan) {
   return PSTM_OK;
 }
 
+pstm_status pstm_copy_trace_columns(float* dst, const float* src, int64_t n_samples,
+                                   int64_t n_traces, int64_t first, int64_t count,
+                                   void* stream) {
+  if (n_samples < 0 || n_traces < 0 || first < 0 || count < 0 || first + count > n_traces ||
+      (n_samples > 0 && count > 0 && (!dst || !src)))
+    return fail(PSTM_EINVAL, "pstm_copy_trace_columns: bad arguments");
+  if (n_samples == 0 || count == 0) return PSTM_OK;
+  CUDA_TRY(cudaMemcpy2DAsync(dst, (size_t)count * sizeof(float), src + first,
+                             (size_t)n_traces * sizeof(float), (size_t)count * sizeof(float),
+                             (size_t)n_samples, cudaMemcpyHostToDevice,
+                             reinterpret_cast<cudaStream_t>(stream)));
+  return PSTM_OK;
+}
+
 pstm_status pstm_trim_memory(int64_t keep_bytes) {
   if (keep_bytes < 0) return fail(PSTM_EINVAL, "keep_bytes must be >= 0");
   int dev = 0;

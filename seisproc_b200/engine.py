@@ -72,6 +72,10 @@ class MigrationEngine:
         self.last_stats = {}
         self._stage, self._stage_key, self._pool = [], None, None
         self._copy_stream = None
+        # bins of at least 2 x block_traces traces are uploaded and migrated in
+        # up to max_blocks blocks (one plan each), pipelining the copies
+        self.block_traces = 100_000
+        self.max_blocks = 4
 
     def migrate_bin_full(
         self,
@@ -115,12 +119,31 @@ class MigrationEngine:
             raise ValueError(f"traces must be (n_samples, n_traces), got {traces.shape}")
         n_s, n_tr = traces.shape
 
-        def upload(stream):
-            # the host array must outlive the asynchronous copy: it is returned
-            host_tr = np.ascontiguousarray(traces, dtype=np.float32)
-            with torch.cuda.stream(stream):
-                tr = torch.from_numpy(host_tr).to(self.device, non_blocking=True)
-            return (lambda: tr), False, host_tr
+        host_tr = np.ascontiguousarray(traces, dtype=np.float32)
+
+        def upload(stream, blocks):
+            # one strided copy per block of traces, each with its own event, so
+            # block b can be migrated while the later blocks are in flight; the
+            # host array outlives the copies (the call ends synchronised)
+            from . import _lib
+            L = _lib.lib()
+            waits = []
+            for first, count in blocks:
+                with torch.cuda.stream(stream):
+                    dst = torch.empty((n_s, count), dtype=torch.float32, device=self.device)
+                    _lib.check(L.pstm_copy_trace_columns(
+                        dst.data_ptr(), host_tr.ctypes.data, n_s, n_tr, first, count,
+                        stream.cuda_stream))
+                    ev = torch.cuda.Event()
+                    ev.record(stream)
+
+                def wait(dst=dst, ev=ev):
+                    cur = torch.cuda.current_stream(self.device)
+                    cur.wait_event(ev)
+                    dst.record_stream(cur)
+                    return dst, False
+                waits.append(wait)
+            return waits
 
         return self._migrate(upload, n_s, n_tr, source_x, source_y, receiver_x, receiver_y,
                              origin_x, origin_y, il_spacing, xl_spacing, n_il, n_xl, dt_ms,
@@ -165,18 +188,19 @@ class MigrationEngine:
         """``migrate_bin_full`` with the traces ``trace_numbers`` taken from a
         ``DataReader`` (``read_traces`` -> (n, n_samples); seisio/gather_readers.py:102-142)
         instead of a transposed host array: they stream into device memory
-        through page-locked chunks while the plan is built, and are staged
-        from their trace-major layout.  Coordinates are those of the selected
+        through page-locked chunks while the plans are built (a large bin in
+        blocks, each migrated while the next is read), and are staged from
+        their trace-major layout.  Coordinates are those of the selected
         traces, in the same order."""
         from .ingest import TraceUpload
         require_cuda(kernel_backend if kernel_backend is not None else self.kernel_backend)
         idx = np.asarray(trace_numbers, np.int64)
         n_s, n_tr = int(reader.get_n_samples()), int(idx.size)
 
-        def upload(stream):
+        def upload(stream, blocks):
             up = TraceUpload(reader, idx, self.device, stream, chunk_traces=chunk_traces,
-                             threads=reader_threads)
-            return up.result, True, None
+                             threads=reader_threads, blocks=blocks)
+            return [lambda b=b: (up.block(b), True) for b in range(len(blocks))]
 
         return self._migrate(upload, n_s, n_tr, source_x, source_y, receiver_x, receiver_y,
                              origin_x, origin_y, il_spacing, xl_spacing, n_il, n_xl, dt_ms,
@@ -189,10 +213,21 @@ class MigrationEngine:
                  origin_y, il_spacing, xl_spacing, n_il, n_xl, dt_ms, t_min_ms, n_times,
                  velocity_mps, max_aperture_m, max_angle_deg, normalize, min_fold,
                  progress_callback, enable_profiling, use_time_dependent_aperture,
-                 velocity_model, kernel_backend, antialias, aa_max_halfwidth):
-        """The body shared by the entry points.  ``upload(stream)`` starts the
-        traces' copy on ``stream`` and returns (wait() -> device tensor,
-        trace_major, host buffer to keep alive)."""
+                 velocity_model, kernel_backend, antialias, aa_max_halfwidth, blocks=None):
+        """The body shared by the entry points.  ``upload(stream, blocks)``
+        starts the copies of the blocks of traces (first, count) on ``stream``
+        and returns one wait() -> (device tensor, trace_major) per block, which
+        also orders the current stream after that block's copy.
+
+        A large bin is split into up to four blocks of traces, each with its
+        own plan: the plans are built while the first block is in flight, and
+        block b is migrated while blocks b + 1 ... are uploaded, hiding most of
+        the host-to-device copy behind the kernels.  The partial images and
+        folds are summed on the device."""
+        if blocks is None:
+            n_blk = min(self.max_blocks, max(1, n_tr // self.block_traces))
+            cuts = np.linspace(0, n_tr, n_blk + 1).astype(np.int64)
+            blocks = [(int(a), int(b - a)) for a, b in zip(cuts[:-1], cuts[1:])]
         t_start = time.perf_counter()
         n_t = int(n_times) if n_times is not None else n_s
         if progress_callback:
@@ -200,11 +235,10 @@ class MigrationEngine:
         with torch.cuda.device(self.device):
             cur = torch.cuda.current_stream(self.device)
             # The traces (the bulk of the input) go up on a side stream while the
-            # plan, which needs only the coordinates, is built on this one.
+            # plans, which need only the coordinates, are built on this one.
             if self._copy_stream is None:
                 self._copy_stream = torch.cuda.Stream(self.device)
             self._copy_stream.wait_stream(cur)
-            tr_wait, trace_major, host_keep = upload(self._copy_stream)
             coords = []
             for a in (source_x, source_y, receiver_x, receiver_y):
                 a = np.asarray(a)
@@ -224,29 +258,47 @@ class MigrationEngine:
             else:
                 vel = velocity_at_outputs(velocity_mps, velocity_model, t_ms, col_x, col_y)
                 vel_t = torch.from_numpy(np.ascontiguousarray(vel)).to(self.device)
-            plan = PSTMPlan(*coords, n_il=n_il, n_xl=n_xl, n_times=n_t, origin_x=origin_x,
-                            origin_y=origin_y, il_dx=il_spacing, il_dy=0.0, xl_dx=0.0,
-                            xl_dy=xl_spacing, t0_ms=t_min_ms, dt_ms=dt_ms, n_samples=n_s,
-                            in_t0_ms=t_min_ms, in_dt_ms=dt_ms, max_aperture_m=max_aperture_m,
-                            max_angle_deg=max_angle_deg,
-                            time_dependent_aperture=use_time_dependent_aperture,
-                            storage=self.storage, variant=self.variant,
-                            kernel_backend=kernel_backend or self.kernel_backend,
-                            antialias=antialias, aa_dx=il_spacing, aa_dy=xl_spacing,
-                            aa_max_halfwidth=aa_max_halfwidth, forward_only=True)
+            # The small synchronous uploads (coordinates, velocity) go first: queued
+            # behind the traces on the copy engine they would hold the host until
+            # the whole bin had crossed the bus, and the plans could not be built
+            # meanwhile.
+            waits = upload(self._copy_stream, blocks)
+            kw = dict(n_il=n_il, n_xl=n_xl, n_times=n_t, origin_x=origin_x, origin_y=origin_y,
+                      il_dx=il_spacing, il_dy=0.0, xl_dx=0.0, xl_dy=xl_spacing, t0_ms=t_min_ms,
+                      dt_ms=dt_ms, n_samples=n_s, in_t0_ms=t_min_ms, in_dt_ms=dt_ms,
+                      max_aperture_m=max_aperture_m, max_angle_deg=max_angle_deg,
+                      time_dependent_aperture=use_time_dependent_aperture,
+                      storage=self.storage, variant=self.variant,
+                      kernel_backend=kernel_backend or self.kernel_backend,
+                      antialias=antialias, aa_dx=il_spacing, aa_dy=xl_spacing,
+                      aa_max_halfwidth=aa_max_halfwidth, forward_only=True)
+            plans = []
             try:
+                # every plan is built before the first launch (the builds
+                # synchronise this stream, which is idle until then)
+                for first, count in blocks:
+                    plans.append(PSTMPlan(*[c[first:first + count] for c in coords], **kw))
                 if progress_callback:
                     progress_callback(0.1, "Running Kirchhoff migration...")
                 ev0 = torch.cuda.Event(enable_timing=True)
                 ev1 = torch.cuda.Event(enable_timing=True)
-                tr = tr_wait()
-                cur.wait_stream(self._copy_stream)
-                tr.record_stream(cur)
-                ev0.record()
-                image, fold = plan.migrate(tr, vel_t, trace_major=trace_major)
+                image = fold = None
+                for plan, wait in zip(plans, waits):
+                    tr, trace_major = wait()
+                    if image is None:
+                        ev0.record()
+                    img_b, fold_b = plan.migrate(tr, vel_t, trace_major=trace_major)
+                    if image is None:
+                        image, fold = img_b, fold_b
+                    else:
+                        image.add_(img_b)
+                        fold.add_(fold_b)
                 ev1.record()
-                plan.check()
-                self.last_stats = dict(plan.stats())
+                for plan in plans:
+                    plan.check()
+                self.last_stats = {k: sum(p.stats()[k] for p in plans)
+                                   for k in ("n_traces", "list_entries", "device_bytes")}
+                self.last_stats["blocks"] = len(plans)
                 self.last_stats["kernel_ms"] = ev0.elapsed_time(ev1)
                 if enable_profiling:
                     pairs = float(fold.double().sum().item())
@@ -255,7 +307,8 @@ class MigrationEngine:
                                 n_tr, pairs, self.last_stats["kernel_ms"],
                                 pairs / max(self.last_stats["kernel_ms"], 1e-9) / 1e6)
             finally:
-                plan.close()
+                for plan in plans:
+                    plan.close()
             if progress_callback:
                 progress_callback(0.9, "Normalizing...")
             if normalize:

@@ -97,21 +97,26 @@ class SegyDataReader(DataReader):
 
 
 class TraceUpload:
-    """Streams ``reader``'s traces ``trace_numbers`` into an (n, n_samples)
-    float32 device tensor on ``stream``, in the background: host threads fill
-    one page-locked chunk while the other is being copied.  ``result()`` waits
-    and orders the caller's current stream after the copies."""
+    """Streams ``reader``'s traces ``trace_numbers`` into (count, n_samples)
+    float32 device tensors on ``stream``, in the background, one per block
+    (first, count) of ``trace_numbers`` (default: one block): host threads fill
+    one page-locked chunk while the other is being copied.  ``block(b)`` waits
+    for block b and orders the caller's current stream after its copies, so
+    block b can be used while the later blocks are still being read."""
 
     def __init__(self, reader: DataReader, trace_numbers: np.ndarray, device: torch.device,
-                 stream: torch.cuda.Stream, chunk_traces: int = 16384, threads: int = 8):
+                 stream: torch.cuda.Stream, chunk_traces: int = 16384, threads: int = 8,
+                 blocks=None):
         self.reader = reader
         self.idx = np.asarray(trace_numbers, np.int64)
         self.device = torch.device(device)
         self.stream = stream
         self.chunk = max(1, int(chunk_traces))
         self.threads = max(1, int(threads))
+        self.blocks = list(blocks) if blocks is not None else [(0, int(self.idx.size))]
+        self._done = [cf.Future() for _ in self.blocks]
         self._pool = cf.ThreadPoolExecutor(max_workers=self.threads + 1)
-        self._job = self._pool.submit(self._run)
+        self._pool.submit(self._run)
 
     def _fill(self, buf: np.ndarray, sel: np.ndarray) -> None:
         """Read ``sel`` into ``buf`` on the pool's threads, split by traces."""
@@ -124,38 +129,53 @@ class TraceUpload:
         for j in jobs:
             j.result()
 
-    def _run(self) -> torch.Tensor:
-        n, n_s = self.idx.size, int(self.reader.get_n_samples())
-        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
-            out = torch.empty((n, n_s), dtype=torch.float32, device=self.device)
-            if n == 0:
-                return out
-            m = min(self.chunk, n)
-            bufs = [torch.empty((m, n_s), dtype=torch.float32, pin_memory=True)
-                    for _ in range(2 if n > m else 1)]
-            done = [None] * len(bufs)
-            starts = list(range(0, n, m))
-            for ci, c0 in enumerate(starts):
-                b = ci % len(bufs)
-                c1 = min(c0 + m, n)
-                if done[b] is not None:
-                    done[b].synchronize()  # the copy out of this buffer has finished
-                self._fill(bufs[b].numpy(), self.idx[c0:c1])
-                out[c0:c1].copy_(bufs[b][:c1 - c0], non_blocking=True)
-                done[b] = torch.cuda.Event()
-                done[b].record(self.stream)
-            # the pinned buffers go back to torch's host cache once the copies end
-            for e in done:
-                e.synchronize()
+    def _run(self) -> None:
+        try:
+            n_s = int(self.reader.get_n_samples())
+            with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+                m = max(1, min(self.chunk, max(c for _, c in self.blocks)))
+                bufs = [torch.empty((m, n_s), dtype=torch.float32, pin_memory=True)
+                        for _ in range(2)]
+                used = [None, None]  # the copy that last read each buffer
+                k = 0
+                for bi, (first, count) in enumerate(self.blocks):
+                    out = torch.empty((count, n_s), dtype=torch.float32, device=self.device)
+                    for c0 in range(0, count, m):
+                        c1 = min(c0 + m, count)
+                        b = k % 2
+                        k += 1
+                        if used[b] is not None:
+                            used[b].synchronize()  # its previous copy has finished
+                        self._fill(bufs[b].numpy(), self.idx[first + c0:first + c1])
+                        out[c0:c1].copy_(bufs[b][:c1 - c0], non_blocking=True)
+                        used[b] = torch.cuda.Event()
+                        used[b].record(self.stream)
+                    ready = torch.cuda.Event()
+                    ready.record(self.stream)
+                    self._done[bi].set_result((out, ready))
+                # the pinned buffers go back to torch's host cache once the copies end
+                for e in used:
+                    if e is not None:
+                        e.synchronize()
+        except BaseException as exc:  # reported by block()
+            for f in self._done:
+                if not f.done():
+                    f.set_exception(exc)
+        finally:
+            self._pool.shutdown(wait=False)
+
+    def block(self, b: int) -> torch.Tensor:
+        out, ready = self._done[b].result()
+        cur = torch.cuda.current_stream(self.device)
+        cur.wait_event(ready)
+        out.record_stream(cur)
         return out
 
     def result(self) -> torch.Tensor:
-        out = self._job.result()
-        self._pool.shutdown(wait=False)
-        cur = torch.cuda.current_stream(self.device)
-        cur.wait_stream(self.stream)
-        out.record_stream(cur)
-        return out
+        """All the traces (a one-block upload)."""
+        if len(self.blocks) != 1:
+            raise ValueError("result() is for a one-block upload; use block(b)")
+        return self.block(0)
 
 
 def upload_traces(reader: DataReader, trace_numbers: np.ndarray,

@@ -21,8 +21,9 @@ def _kw(s):
                 max_angle_deg=s.max_angle_deg, normalize=True, velocity_model=s.vrms)
 
 
+@pytest.mark.parametrize("blocks", [1, 3])
 @pytest.mark.parametrize("kind", ["numpy", "segy"])
-def test_reader_path_equals_array_path(tmp_path, kind):
+def test_reader_path_equals_array_path(tmp_path, kind, blocks):
     from seisproc_b200 import ingest as I
     from seisproc_b200 import velocity_io as V
     from seisproc_b200.engine import MigrationEngine
@@ -38,9 +39,34 @@ def test_reader_path_equals_array_path(tmp_path, kind):
     idx = np.sort(rs.choice(s.n_traces, 3700, replace=False))  # one bin's traces
     coords = [np.asarray(a)[idx] for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
     eng = MigrationEngine()
+    if blocks > 1:
+        eng.block_traces = idx.size // blocks  # both paths split the bin the same way
     img_r, fold_r = eng.migrate_bin_from_reader(reader, idx, *coords, chunk_traces=1000,
                                                 reader_threads=3, **_kw(s))
+    assert eng.last_stats["blocks"] == blocks
     img_a, fold_a = eng.migrate_bin_full(reader.read_traces(idx).T, *coords, **_kw(s))
     assert np.array_equal(fold_r, fold_a)
     assert np.array_equal(img_r, img_a)
     assert np.abs(img_a).max() > 0
+
+
+def test_block_pipelined_upload_matches_single_plan():
+    """A bin split into blocks of traces (one plan each, uploads pipelined
+    against the migrations, partial images summed) gives the single-plan image
+    to float rounding and the same fold."""
+    from seisproc_b200.engine import MigrationEngine
+    s = _survey()
+    tr = s.traces.cpu().numpy()
+    host = torch.empty(tr.shape, dtype=torch.float32, pin_memory=True)
+    host.copy_(torch.from_numpy(tr))
+    coords = (s.source_x, s.source_y, s.receiver_x, s.receiver_y)
+    eng = MigrationEngine()
+    one, f1 = eng.migrate_bin_full(host.numpy(), *coords, **_kw(s))
+    assert eng.last_stats["blocks"] == 1
+    eng.block_traces = 1200  # 5000 traces -> 4 blocks
+    four, f4 = eng.migrate_bin_full(host.numpy(), *coords, **_kw(s))
+    assert eng.last_stats["blocks"] == 4
+    four_pageable, _ = eng.migrate_bin_full(tr, *coords, **_kw(s))
+    assert np.array_equal(f1, f4)
+    assert np.linalg.norm(four - one) <= 1e-6 * np.linalg.norm(one)
+    assert np.array_equal(four, four_pageable)
