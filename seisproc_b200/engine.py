@@ -256,12 +256,18 @@ class MigrationEngine:
                 vel_t = velocity_grid(velocity_model, np.asarray(t_ms, np.float64) / 1000.0,
                                       col_x, col_y, self.device)
             else:
-                vel = velocity_at_outputs(velocity_mps, velocity_model, t_ms, col_x, col_y)
-                vel_t = torch.from_numpy(np.ascontiguousarray(vel)).to(self.device)
-            # The small synchronous uploads (coordinates, velocity) go first: queued
-            # behind the traces on the copy engine they would hold the host until
-            # the whole bin had crossed the bus, and the plans could not be built
-            # meanwhile.
+                vel = np.ascontiguousarray(
+                    velocity_at_outputs(velocity_mps, velocity_model, t_ms, col_x, col_y))
+                # on the copy stream ahead of the traces (asynchronous from
+                # page-locked memory; ``vel`` lives until the call returns)
+                with torch.cuda.stream(self._copy_stream):
+                    vel_t = torch.from_numpy(vel).to(self.device, non_blocking=True)
+                vel_t.record_stream(cur)
+            # The small uploads (coordinates, velocity) go first: queued behind the
+            # traces on the copy engine, a synchronous one would hold the host
+            # until the whole bin had crossed the bus, and the plans could not be
+            # built meanwhile.  Block 0's event follows the velocity's copy on the
+            # copy stream, so the first migration waits for both.
             waits = upload(self._copy_stream, blocks)
             kw = dict(n_il=n_il, n_xl=n_xl, n_times=n_t, origin_x=origin_x, origin_y=origin_y,
                       il_dx=il_spacing, il_dy=0.0, xl_dx=0.0, xl_dy=xl_spacing, t0_ms=t_min_ms,
