@@ -111,6 +111,13 @@ typedef struct pstm_params {
                                   (demigration, V-gradient, batches and the anti-alias
                                   filter refuse it); the fold still counts hard-masked
                                   pairs.  The offset taper is per trace: scale the traces. */
+  double ray_gradient;         /* 0: straight rays, t = (r_s + r_r) / V (DSR).  k != 0: rays
+                                  in v(z) = v0 + k z, one-way time arccosh(1 + k r^2 /
+                                  (2 v0 z)) / k, v0 = the velocity passed (constant), z =
+                                  v0 t0 / 2: the traveltime table the reference migrator
+                                  interpolates by default (traveltime_lut.py:141-167,
+                                  kirchhoff_migrator.py:146-175, 346-365).  Float32,
+                                  migration only, like taper_width (and not with it). */
 } pstm_params;
 
 typedef struct pstm_geometry {

@@ -56,8 +56,18 @@ def _as_vgrid(velocity, n_t: int, n_c: int) -> np.ndarray:
     return v.reshape(n_t, n_c)
 
 
+def curved_ray_time_s(h, z, v0, k):
+    """One-way traveltime (s) in v(z) = v0 + k z along the circular ray,
+    arccosh(1 + k r^2 / (2 v0 z)) / k with z floored at 1e-6 m: the reference's
+    traveltime table for a velocity gradient (traveltime_lut.py:141-167), which
+    the KirchhoffMigrator interpolates bilinearly by default."""
+    zs = np.maximum(z, 1e-6)
+    arg = np.maximum(1.0 + k * (h * h + zs * zs) / (2.0 * v0 * zs), 1.0)
+    return np.arccosh(arg) / k
+
+
 def _column_terms(xc, yc, sx, sy, rx, ry, z, v, t_out_ms, n_s, in_dt_ms, in_t0_ms, aperture,
-                  angle_rad, time_dependent, weight, clamp):
+                  angle_rad, time_dependent, weight, clamp, ray_gradient=0.0):
     """All per-(trace, t0) quantities for one output column.  Shapes (n_tr, n_t)."""
     hs = np.hypot(xc - sx, yc - sy)[:, None]
     hr = np.hypot(xc - rx, yc - ry)[:, None]
@@ -74,7 +84,11 @@ def _column_terms(xc, yc, sx, sy, rx, ry, z, v, t_out_ms, n_s, in_dt_ms, in_t0_m
            (np.arctan2(hr, zang) < angle_rad)
     rs = np.sqrt(hs * hs + zz * zz)
     rr = np.sqrt(hr * hr + zz * zz)
-    t_ms = (rs + rr) * 1000.0 / v[None, :]
+    if ray_gradient:
+        t_ms = 1000.0 * (curved_ray_time_s(hs, zz, v[None, :], ray_gradient) +
+                         curved_ray_time_s(hr, zz, v[None, :], ray_gradient))
+    else:
+        t_ms = (rs + rr) * 1000.0 / v[None, :]
     if clamp == "migrator":
         idx = np.clip(t_ms / in_dt_ms, 0.0, n_s - 2)
     else:
@@ -197,7 +211,7 @@ def triangle_explicit(tr: np.ndarray, i: int, L: int) -> float:
 def migrate_fp64(traces, sx, sy, rx, ry, out_x, out_y, t_out_ms, velocity, in_dt_ms,
                  in_t0_ms, aperture, angle_deg, time_dependent=False,
                  weight="obliquity_spreading", clamp="full", antialias=False, dx_out=0.0,
-                 dy_out=0.0, l_max=32.0, columns=None, taper_width=0.0):
+                 dy_out=0.0, l_max=32.0, columns=None, taper_width=0.0, ray_gradient=0.0):
     """Forward migration (data -> image) in float64.
 
     traces: (N_s, N_tr); coordinates float64 (any common origin);
@@ -208,6 +222,8 @@ def migrate_fp64(traces, sx, sy, rx, ry, out_x, out_y, t_out_ms, velocity, in_dt
     (others stay 0).  ``taper_width`` > 0 multiplies every weight by the
     aperture controller's distance and angle cosine tapers of both legs
     (``aperture_taper_fp64``); the fold still counts the hard-masked pairs.
+    ``ray_gradient`` k != 0 replaces the straight-ray traveltime by the curved
+    ray of v(z) = v0 + k z (``curved_ray_time_s``), v0 = ``velocity`` (constant).
     """
     tr = np.asarray(traces, dtype=np.float64)
     n_s, n_tr = tr.shape
@@ -236,7 +252,7 @@ def migrate_fp64(traces, sx, sy, rx, ry, out_x, out_y, t_out_ms, velocity, in_dt
             continue
         mask, rs, rr, hs, hr, idx, w, _ = _column_terms(
             out_x[c], out_y[c], sx[cand], sy[cand], rx[cand], ry[cand], z, v, t_out_ms, n_s,
-            in_dt_ms, in_t0_ms, aperture, ang, time_dependent, weight, clamp)
+            in_dt_ms, in_t0_ms, aperture, ang, time_dependent, weight, clamp, ray_gradient)
         if taper_width > 0:
             w = w * aperture_taper_fp64(hs, hr, z[None, :], aperture, ang, taper_width)
         keep = np.nonzero(mask.any(axis=1))[0]

@@ -37,7 +37,7 @@ class Params(C.Structure):
                 ("clamp", C.c_int32), ("storage", C.c_int32), ("antialias", C.c_int32),
                 ("aa_dx", C.c_double), ("aa_dy", C.c_double), ("aa_max_halfwidth", C.c_double),
                 ("variant", C.c_int32), ("forward_only", C.c_int32),
-                ("taper_width", C.c_double)]
+                ("taper_width", C.c_double), ("ray_gradient", C.c_double)]
 
 
 class Geometry(C.Structure):

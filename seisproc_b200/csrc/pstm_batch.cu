@@ -148,10 +148,10 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
       free_batch(b);
       return bfail(PSTM_ENOTSUP, "the batched launch is built for the plain operator");
     }
-    if (p->params.taper_width > 0) {
+    if (p->params.taper_width > 0 || p->params.ray_gradient != 0) {
       free_batch(b);
-      return bfail(PSTM_ENOTSUP, "the batched launch applies no aperture taper: build the "
-                                 "class plans without taper_width");
+      return bfail(PSTM_ENOTSUP, "the batched launch applies no aperture taper or curved rays: "
+                                 "build the class plans without taper_width or ray_gradient");
     }
     if (p->params.forward_only && p->params.storage == PSTM_F32) {
       free_batch(b);

@@ -49,6 +49,9 @@ struct KArgs {
   int aa_pad;
   int row_origin;  // expanded rows: intercept origin (entry index)
   TaperArgs tp;    // plans built with a taper width
+  // curved rays (plans built with a ray gradient k): k, and 1000 / (k in_dt)
+  // turning the summed arccosh of the two legs into an input sample index
+  float cr_k, cr_scale;
 };
 
 __device__ __forceinline__ float vel_at(const KArgs& A, int k, int c) {
@@ -201,6 +204,10 @@ inline KArgs make_args(const Plan* p, const float* vel, int64_t vst, int64_t vsc
     A.tp.amax = (float)th;
     A.tp.tan2 = (float)(std::tan(a0) * std::tan(a0));
   }
+  A.cr_k = (float)p->params.ray_gradient;
+  A.cr_scale = p->params.ray_gradient != 0
+                   ? (float)(1000.0 / (p->params.ray_gradient * p->params.in_dt_ms))
+                   : 0.0f;
   return A;
 }
 

@@ -100,13 +100,16 @@ __device__ __forceinline__ float lds_elem<__half>(uint32_t addr) {
 // MASKED) and, for f16 storage, its scale.  A MASKED sweep starts at group g0,
 // the first 64-sample group holding a contributing sample of any of its traces
 // (warp-uniform, so the skipped groups cost one uniform branch each).
-template <int M, typename ST, int WM, bool LOWC, bool MASKED, int OP, int NTR, bool TAPER>
+template <int M, typename ST, int WM, bool LOWC, bool MASKED, int OP, int NTR, bool TAPER,
+          bool CURVED = false>
 __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], const f2 (&aa)[M],
                                              const float (&hs2)[NTR], const float (&hr2)[NTR],
                                              const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
                                              const float (&sc)[NTR], f2 bb, f2 magic2,
                                              float hi_c, float lo_c, int kw, int lane, int g0,
-                                             const TaperArgs& tp) {
+                                             const TaperArgs& tp, float cr_scale = 0.f) {
+  // curved rays: zz = z^2 + f, aa = k / (2 v0 max(z, 1e-6)); no pre-scaling
+  constexpr bool PRE = kPrescaled<OP, WM> && !CURVED;
   constexpr int ES = (int)sizeof(ST);
   constexpr int SHIFT = ES == 8 ? 3 : (ES == 4 ? 2 : 1);
 #pragma unroll
@@ -118,7 +121,18 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
     for (int n = 0; n < NTR; ++n) {
       const f2 hs2b = f2_bcast(hs2[n]), hr2b = f2_bcast(hr2[n]);
       f2 rrs, rrr, qs, qr, id;
-      if constexpr (kPrescaled<OP, WM>) {
+      if constexpr (CURVED) {
+        // one-way times in v(z) = v0 + k z: arccosh(1 + k r^2 / (2 v0 z)) / k
+        rrs = f2_add(hs2b, zz[i]);
+        rrr = f2_add(hr2b, zz[i]);
+        qs = f2{rsqrt_approx(rrs.x), rsqrt_approx(rrs.y)};
+        qr = f2{rsqrt_approx(rrr.x), rsqrt_approx(rrr.y)};
+        const f2 xs = f2_fma(rrs, aa[i], f2_bcast(1.0f));
+        const f2 xr = f2_fma(rrr, aa[i], f2_bcast(1.0f));
+        const f2 tt = f2{acoshf(fmaxf(xs.x, 1.0f)) + acoshf(fmaxf(xr.x, 1.0f)),
+                         acoshf(fmaxf(xs.y, 1.0f)) + acoshf(fmaxf(xr.y, 1.0f))};
+        id = f2_fma(tt, f2_bcast(cr_scale), bb);
+      } else if constexpr (PRE) {
         // zz = a^2 (z^2 + eps), aa = a^2: rr' = a^2 rr, q' = q / a, and
         // rr'_s q'_s + rr'_r q'_r = a (r_s + r_r), the index less its offset
         rrs = f2_fma(hs2b, aa[i], zz[i]);
@@ -164,7 +178,7 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
         amp = f2_fma(fr, dx, x0);
       }
       const f2 p = f2_mul(qs, qr);
-      if constexpr (kPrescaled<OP, WM>) {
+      if constexpr (PRE) {
         // weight p^2 (obliquity x spreading; the a^4 z^2 factor comes in the
         // epilogue), p (obliquity) or 1; formed while the taps load
         f2 w = p;
@@ -292,7 +306,7 @@ __device__ __forceinline__ void sweep_aa(f2 (&acc)[M], const f2 (&zz)[M], const 
 }
 
 template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP, bool AA = false,
-          bool TAPER = false>
+          bool TAPER = false, bool CURVED = false>
 __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, const int win,
                                             unsigned char* smem) {
   constexpr int NW = COLS * WPC;
@@ -388,7 +402,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     const float zh = depth_of(vh, out_time_ms(kh, A.out_dt, A.out_t0));
     zz[i] = f2{fmaf(zl, zl, kRadicandFloor), fmaf(zh, zh, kRadicandFloor)};
     aa[i] = f2{1000.0f / (vl * A.in_dt), 1000.0f / (vh * A.in_dt)};
-    if constexpr (kPrescaled<OP, WM>) {
+    if constexpr (CURVED) {
+      // aa holds k / (2 v0 max(z, 1e-6)) for the curved-ray argument
+      aa[i] = f2{A.cr_k / (2.0f * vl * fmaxf(zl, 1e-6f)), A.cr_k / (2.0f * vh * fmaxf(zh, 1e-6f))};
+    } else if constexpr (kPrescaled<OP, WM>) {
       aa[i] = f2_mul(aa[i], aa[i]);
       zz[i] = f2_mul(zz[i], aa[i]);
     }
@@ -507,12 +524,14 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const uint32_t rb[2] = {rb0, rb0 + (uint32_t)RP};
         const int kk[2] = {ka, kb};
         if (ka > kw || kb > kw)
-          sweep_traces<M, ST, WM, LOWC, true, OP, 2, TAPER>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
+          sweep_traces<M, ST, WM, LOWC, true, OP, 2, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
                                                              hi_c, lo_c, kw, lane,
-                                                             (min(ka, kb) - kw) >> 6, A.tp);
+                                                             (min(ka, kb) - kw) >> 6, A.tp,
+                                                             A.cr_scale);
         else
-          sweep_traces<M, ST, WM, LOWC, false, OP, 2, TAPER>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
-                                                              hi_c, lo_c, kw, lane, 0, A.tp);
+          sweep_traces<M, ST, WM, LOWC, false, OP, 2, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
+                                                              hi_c, lo_c, kw, lane, 0, A.tp,
+                                                              A.cr_scale);
       } else if (la || lb) {
         const int u = la ? t : t + 1;
         const float hs[1] = {__shfl_sync(0xffffffffu, hs2, u)};
@@ -521,12 +540,13 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const uint32_t rb[1] = {la ? rb0 : rb0 + (uint32_t)RP};
         const int kk[1] = {la ? ka : kb};
         if (kk[0] > kw)
-          sweep_traces<M, ST, WM, LOWC, true, OP, 1, TAPER>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
+          sweep_traces<M, ST, WM, LOWC, true, OP, 1, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
                                                              hi_c, lo_c, kw, lane, (kk[0] - kw) >> 6,
-                                                             A.tp);
+                                                             A.tp, A.cr_scale);
         else
-          sweep_traces<M, ST, WM, LOWC, false, OP, 1, TAPER>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
-                                                              hi_c, lo_c, kw, lane, 0, A.tp);
+          sweep_traces<M, ST, WM, LOWC, false, OP, 1, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
+                                                              hi_c, lo_c, kw, lane, 0, A.tp,
+                                                              A.cr_scale);
       }
       const int adv = pair ? 2 : 1;
       t += adv;
@@ -598,7 +618,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
       const float zh = depth_of(vh, out_time_ms(kh, A.out_dt, A.out_t0));
       fl = zl * zl;
       fh = zh * zh;
-      if constexpr (kPrescaled<OP, WM>) {
+      if constexpr (kPrescaled<OP, WM> && !CURVED) {
         // the pre-scaled weight p' = p / a^2: multiply by a^4 (p^2) or a^2 (p)
         const float al = 1000.0f / (vl * A.in_dt), ah = 1000.0f / (vh * A.in_dt);
         const float al2 = al * al, ah2 = ah * ah;
@@ -616,10 +636,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
 }
 
 template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP, bool AA = false,
-          bool TAPER = false>
+          bool TAPER = false, bool CURVED = false>
 __global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const KArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
-  gather_tile<COLS, WPC, M, ST, WM, LOWC, OP, AA, TAPER>(A, blockIdx.x, blockIdx.y, smem);
+  gather_tile<COLS, WPC, M, ST, WM, LOWC, OP, AA, TAPER, CURVED>(A, blockIdx.x, blockIdx.y, smem);
 }
 
 // Persistent batched kernel: CTAs pull (class, tile, window) work items from a
@@ -653,10 +673,11 @@ __global__ void __launch_bounds__(COLS* WPC * 32, 1)
 }
 
 template <int COLS, int WPC, int M, typename ST, int WM, int OP, bool AA = false,
-          bool TAPER = false>
+          bool TAPER = false, bool CURVED = false>
 inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
-  auto kern = needs_lowclamp(p) ? pstm_gather2_kernel<COLS, WPC, M, ST, WM, true, OP, AA, TAPER>
-                                : pstm_gather2_kernel<COLS, WPC, M, ST, WM, false, OP, AA, TAPER>;
+  auto kern = needs_lowclamp(p)
+                  ? pstm_gather2_kernel<COLS, WPC, M, ST, WM, true, OP, AA, TAPER, CURVED>
+                  : pstm_gather2_kernel<COLS, WPC, M, ST, WM, false, OP, AA, TAPER, CURVED>;
   const int T = WPC * 64 * M;
   KArgs A2 = A;
   if (!ring_shape(COLS, T, p->row_stride, (int)sizeof(ST), &A2.ring_stages, &A2.ring_rows))
@@ -671,24 +692,24 @@ inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int COLS, int WPC, int M, typename ST, int OP, bool TAPER = false>
+template <int COLS, int WPC, int M, typename ST, int OP, bool TAPER = false, bool CURVED = false>
 inline cudaError_t dispatch2_wm(const Plan* p, const KArgs& A, cudaStream_t s) {
   const int wm = p->params.weight;
   constexpr bool k32 = std::is_same<ST, float>::value || std::is_same<ST, float2>::value ||
                       std::is_same<ST, RowIcpt>::value;
   if constexpr (OP == OP_VGRAD || !k32) {
     if (wm != W_OBL_SPREAD) return cudaErrorNotSupported;
-    return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP, false, TAPER>(p, A, s);
+    return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP, false, TAPER, CURVED>(p, A, s);
   } else {
     switch (wm) {
       case W_OBL_SPREAD:
-        return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP, false, TAPER>(p, A, s);
+        return launch2_one<COLS, WPC, M, ST, W_OBL_SPREAD, OP, false, TAPER, CURVED>(p, A, s);
       case W_SPREAD:
-        return launch2_one<COLS, WPC, M, ST, W_SPREAD, OP, false, TAPER>(p, A, s);
+        return launch2_one<COLS, WPC, M, ST, W_SPREAD, OP, false, TAPER, CURVED>(p, A, s);
       case W_OBL:
-        return launch2_one<COLS, WPC, M, ST, W_OBL, OP, false, TAPER>(p, A, s);
+        return launch2_one<COLS, WPC, M, ST, W_OBL, OP, false, TAPER, CURVED>(p, A, s);
       case W_NONE:
-        return launch2_one<COLS, WPC, M, ST, W_NONE, OP, false, TAPER>(p, A, s);
+        return launch2_one<COLS, WPC, M, ST, W_NONE, OP, false, TAPER, CURVED>(p, A, s);
     }
     return cudaErrorInvalidValue;
   }
@@ -700,6 +721,9 @@ cudaError_t launch_forward_icpt(const Plan* p, const KArgs& A, cudaStream_t s);
 // Forward launch with the aperture tapers (float32 plans with a taper width),
 // instantiated in pstm_gather_fwd_taper.cu.
 cudaError_t launch_forward_taper(const Plan* p, const KArgs& A, cudaStream_t s);
+// Forward launch with curved-ray traveltimes (float32 plans with a ray
+// gradient), instantiated in pstm_gather_fwd_taper.cu as well.
+cudaError_t launch_forward_curved(const Plan* p, const KArgs& A, cudaStream_t s);
 
 template <int COLS, int WPC, int M, int OP>
 inline cudaError_t dispatch2_st(const Plan* p, const KArgs& A, cudaStream_t s) {
@@ -717,6 +741,12 @@ inline cudaError_t dispatch2_st(const Plan* p, const KArgs& A, cudaStream_t s) {
       if (p->params.taper_width > 0) {
         if constexpr (OP == OP_FWD)
           return launch_forward_taper(p, A, s);
+        else
+          return cudaErrorNotSupported;
+      }
+      if (p->params.ray_gradient != 0) {
+        if constexpr (OP == OP_FWD)
+          return launch_forward_curved(p, A, s);
         else
           return cudaErrorNotSupported;
       }

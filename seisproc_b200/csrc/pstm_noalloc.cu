@@ -209,8 +209,9 @@ extern "C" pstm_status pstm_migrate_noalloc(const pstm_grid* grid, const pstm_pa
     return noalloc_fail(PSTM_EINVAL, "invalid grid or migration parameters");
   if (params->storage != PSTM_F32 || params->antialias)
     return noalloc_fail(PSTM_EINVAL, "the no-allocation entry point stages float32 traces only");
-  if (params->taper_width != 0.0)
-    return noalloc_fail(PSTM_EINVAL, "the no-allocation entry point applies no aperture taper");
+  if (params->taper_width != 0.0 || params->ray_gradient != 0.0)
+    return noalloc_fail(PSTM_EINVAL, "the no-allocation entry point applies no aperture taper "
+                                     "or curved rays");
   if (geometry->coord_dtype != PSTM_F32 && geometry->coord_dtype != PSTM_F64)
     return noalloc_fail(PSTM_EINVAL, "coordinates must be F32 or F64");
   const int64_t n = geometry->n_traces;

@@ -662,6 +662,12 @@ static pstm_status validate(const pstm_grid* g, const pstm_params* prm, const ps
   if (prm->taper_width > 0 && (prm->storage != PSTM_F32 || prm->antialias))
     return fail(PSTM_ENOTSUP, "the aperture taper is built for float32 storage without the "
                               "anti-alias filter");
+  if (!std::isfinite(prm->ray_gradient))
+    return fail(PSTM_EINVAL, "ray_gradient must be finite");
+  if (prm->ray_gradient != 0 &&
+      (prm->storage != PSTM_F32 || prm->antialias || prm->taper_width > 0))
+    return fail(PSTM_ENOTSUP, "curved rays (ray_gradient) are built for float32 storage "
+                              "without the anti-alias filter or the aperture taper");
   if (prm->antialias && prm->weight != PSTM_WEIGHT_OBLIQUITY_SPREADING)
     return fail(PSTM_ENOTSUP, "the anti-alias kernel is built for the obliquity x spreading weight");
   if (geo->n_traces < 0 || geo->n_traces > (int64_t)INT32_MAX)
@@ -743,12 +749,13 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
   }
   if (!shape_for_variant(prm->variant, g->n_xl, g->n_times, &p->shape))
     return fail(PSTM_EINVAL, "unknown kernel variant");
-  if (prm->taper_width > 0) {
-    // the tapered kernel is built for the 16-column shapes only
+  if (prm->taper_width > 0 || prm->ray_gradient != 0) {
+    // the tapered and curved-ray kernels are built for the 16-column shapes only
     if (prm->variant == 0) {
       shape_for_variant(g->n_xl < 2 ? 9 : 3, g->n_xl, g->n_times, &p->shape);
     } else if (p->shape.id != 3 && p->shape.id != 9) {
-      return fail(PSTM_ENOTSUP, "the aperture taper runs kernel variants 3 and 9 only");
+      return fail(PSTM_ENOTSUP,
+                  "the aperture taper and curved rays run kernel variants 3 and 9 only");
     }
   }
   p->tiles_il = (g->n_il + p->shape.tile_il - 1) / p->shape.tile_il;
@@ -1059,8 +1066,9 @@ pstm_status pstm_demigrate(pstm_plan* plan, const float* image, const float* vel
   Plan* p = reinterpret_cast<Plan*>(plan);
   if (p->params.antialias)
     return fail(PSTM_ENOTSUP, "demigration is built for the plain (non-anti-aliased) operator");
-  if (p->params.taper_width > 0)
-    return fail(PSTM_ENOTSUP, "demigration needs a plan built without taper_width");
+  if (p->params.taper_width > 0 || p->params.ray_gradient != 0)
+    return fail(PSTM_ENOTSUP, "demigration needs a plan built without taper_width or "
+                              "ray_gradient");
   pstm_status st = check_velocity_args(vel, vst, vsc);
   if (st != PSTM_OK) return st;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -1097,8 +1105,9 @@ pstm_status pstm_velocity_gradient(pstm_plan* plan, const float* grad_image, con
                               "operator");
   if (p->params.forward_only && p->params.storage == PSTM_F32)
     return fail(PSTM_ENOTSUP, "velocity gradient needs a plan built without forward_only");
-  if (p->params.taper_width > 0)
-    return fail(PSTM_ENOTSUP, "velocity gradient needs a plan built without taper_width");
+  if (p->params.taper_width > 0 || p->params.ray_gradient != 0)
+    return fail(PSTM_ENOTSUP, "velocity gradient needs a plan built without taper_width or "
+                              "ray_gradient");
   pstm_status st = check_velocity_args(vel, vst, vsc);
   if (st != PSTM_OK) return st;
   std::string why;

@@ -72,6 +72,8 @@ class PSTMPlan:
     rather than to float rounding, and ``velocity_gradient`` and batches refuse
     the plan.  ``taper_width`` in (0, 1) adds the aperture controller's
     distance and angle cosine tapers of both legs (migration only, float32).
+    ``ray_gradient`` k != 0 takes curved-ray traveltimes in v(z) = v0 + k z
+    (the velocity passed is v0), as the reference migrator's default table.
     """
 
     def __init__(self, source_x, source_y, receiver_x, receiver_y, *, n_il: int, n_xl: int,
@@ -82,7 +84,8 @@ class PSTMPlan:
                  clamp: str = "full", storage: str = "f32", variant: int = 0,
                  kernel_backend=None, antialias: bool = False, aa_dx: float = 0.0,
                  aa_dy: float = 0.0, aa_max_halfwidth: float = 32.0,
-                 forward_only: bool = False, taper_width: float = 0.0):
+                 forward_only: bool = False, taper_width: float = 0.0,
+                 ray_gradient: float = 0.0):
         require_cuda(kernel_backend)
         self._lib = _lib.lib()
         self._handle = C.c_void_p(None)
@@ -110,7 +113,8 @@ class PSTMPlan:
                                   int(bool(time_dependent_aperture)), WEIGHTS[weight],
                                   CLAMPS[clamp], STORAGES[storage], int(bool(antialias)),
                                   float(aa_dx), float(aa_dy), float(aa_max_halfwidth),
-                                  int(variant), int(bool(forward_only)), float(taper_width))
+                                  int(variant), int(bool(forward_only)), float(taper_width),
+                                  float(ray_gradient))
         geo = _lib.Geometry(n_tr, _lib.PSTM_F64 if dt == torch.float64 else _lib.PSTM_F32,
                             *[c.data_ptr() for c in coords])
         _lib.check(self._lib.pstm_plan_create(C.byref(self._handle), C.byref(self.grid),

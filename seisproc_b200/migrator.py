@@ -14,13 +14,17 @@ kirchhoff_migrator.py:40-592):
   atan2(h, |z| + 1e-6) < theta, per-leg aperture;
 * ``MigrationResult`` with ``apply_fold_normalization`` (:317-349).
 
-Differences, each deliberate: traveltimes are always exact DSR (the reference
-defaults to a bilinear (h, z) lookup table, traveltime_lut.py:250-308, which only
-approximates them); ``config.weight_mode`` is honoured (SPREADING is the
-reference's 1/(r_s r_r + 1e-6); FULL is obliquity x spreading; OBLIQUITY and
+Velocity and traveltimes as the reference: v0 of the model, depth z = v0 t / 2,
+straight rays, or (``use_traveltime_lut=True``, the default) the curved rays of
+its traveltime table when the model has a v(z) gradient -- computed exactly
+where the reference interpolates a bilinear (h, z) table
+(traveltime_lut.py:141-167, 250-308; the images agree to ~1e-5).
+
+Differences, each deliberate: ``config.weight_mode`` is honoured (SPREADING is
+the reference's 1/(r_s r_r + 1e-6); FULL is obliquity x spreading; OBLIQUITY and
 NONE as named) and ``min_offset_m``/``max_offset_m`` select the traces; a
-laterally varying velocity model is used as V_rms(t0, x, y) where the reference
-uses only v0.
+laterally varying velocity model (which the reference cannot migrate with), or
+any model with ``vrms_velocity=True``, is used as V_rms(t0, x, y).
 """
 from __future__ import annotations
 
@@ -33,7 +37,8 @@ import numpy as np
 import torch
 
 from .kernel_backend import require_cuda
-from .models import MigrationConfig, MigrationGeometry, SeismicData, VelocityModel, WeightMode
+from .models import (MigrationConfig, MigrationGeometry, SeismicData, VelocityModel,
+                     VelocityType, WeightMode)
 
 logger = logging.getLogger(__name__)
 
@@ -182,14 +187,19 @@ class KirchhoffMigrator(BaseMigrator):
                  device: Optional[torch.device] = None, use_traveltime_lut: bool = True,
                  kernel_backend=None, storage: str = "f32", variant: int = 0,
                  antialias: bool = False, aa_max_halfwidth: float = 32.0,
-                 aperture_taper: bool = False):
+                 aperture_taper: bool = False, vrms_velocity: bool = False):
         self.velocity = velocity
         require_cuda(kernel_backend)
         self.device = torch.device(device) if device is not None else \
             torch.device("cuda", torch.cuda.current_device())
         if self.device.type != "cuda":
             raise ValueError("KirchhoffMigrator runs on a CUDA device only")
-        self._use_traveltime_lut = use_traveltime_lut  # accepted; traveltimes are exact DSR
+        # The reference's velocity semantics: v0 for every model, z = v0 t / 2,
+        # straight rays; with its default traveltime table a v(z) gradient turns
+        # the rays into arcs (computed exactly here, not interpolated from a
+        # table).  vrms_velocity=True takes the model as V_rms(t0, x, y) instead.
+        self._use_traveltime_lut = use_traveltime_lut
+        self.vrms_velocity = vrms_velocity
         self.kernel_backend = kernel_backend
         self.storage = storage
         self.variant = variant
@@ -215,6 +225,22 @@ class KirchhoffMigrator(BaseMigrator):
         x = (g.x_origin + il * g.d_inline + 0 * xl).ravel()
         y = (g.y_origin + 0 * il + xl * g.d_xline).ravel()
         return x, y
+
+    def _velocity_and_rays(self) -> Tuple[torch.Tensor, float]:
+        """(velocity on the device, ray gradient k) of a migration.  The
+        reference migrator uses v0 alone (kirchhoff_migrator.py:312,
+        migrate_gather :221-224); its default traveltime table bends the rays
+        when the model has a gradient (:146-175, traveltime_lut.py:141-167).
+        Laterally varying models (the reference cannot migrate with them) and
+        ``vrms_velocity`` use the model as V_rms at every output sample."""
+        vm = self.velocity
+        lateral = vm.velocity_type in (VelocityType.V_OF_XZ, VelocityType.V_OF_XYZ)
+        if self.vrms_velocity or lateral or vm.v0 is None:
+            return self._velocity_grid(), 0.0
+        k = float(vm.gradient or 0.0) if self._use_traveltime_lut else 0.0
+        if abs(k) < 1e-10:
+            k = 0.0
+        return torch.full((1,), float(vm.v0), dtype=torch.float32, device=self.device), k
 
     def _velocity_grid(self) -> torch.Tensor:
         """V at the output samples on the device (laterally varying models are
@@ -245,6 +271,11 @@ class KirchhoffMigrator(BaseMigrator):
         full = sel.size == geometry.n_traces
         traces = gather.traces if full else gather.traces[:, sel]
         tw = float(self.config.taper_width) if self.aperture_taper else 0.0
+        v, ray_k = self._velocity_and_rays()
+        if tw > 0 and ray_k != 0:
+            raise NotImplementedError(
+                "aperture tapers with curved rays are not built: pass use_traveltime_lut=False "
+                "(straight rays at v0) or vrms_velocity=True")
         if tw > 0:
             w_off = offset_taper(off[sel], self.config.min_offset_m, self.config.max_offset_m, tw)
             traces = np.asarray(traces, np.float32) * w_off[None, :].astype(np.float32)
@@ -262,9 +293,9 @@ class KirchhoffMigrator(BaseMigrator):
                 weight=_WEIGHT_OF_MODE[self.config.weight_mode], clamp="migrator",
                 storage=self.storage, variant=self.variant, kernel_backend=self.kernel_backend,
                 antialias=self.antialias, aa_dx=g.d_inline, aa_dy=g.d_xline,
-                aa_max_halfwidth=self.aa_max_halfwidth, forward_only=True, taper_width=tw)
+                aa_max_halfwidth=self.aa_max_halfwidth, forward_only=True, taper_width=tw,
+                ray_gradient=ray_k)
             try:
-                v = self._velocity_grid()
                 tr = torch.from_numpy(np.ascontiguousarray(traces, dtype=np.float32))
                 img, fold = plan.migrate(tr.to(self.device), v)
                 plan.check()

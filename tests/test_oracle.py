@@ -225,3 +225,28 @@ def test_aperture_tapers_match_reference_controller():
             got = got * om[:, None]
             assert np.allclose(got, want[q], atol=2e-5), (k, q)
         assert ((want > 0) & (want < 1)).any()  # the tapers are exercised
+
+
+def test_curved_ray_oracle_matches_reference_lut_migrator():
+    """The reference KirchhoffMigrator's default path interpolates a traveltime
+    table (straight rays at v0, or curved rays for a v(z) gradient); the FP64
+    oracle with the exact formulas reproduces its images to the table's
+    interpolation error."""
+    import os
+    from conftest import ROOT
+    g = np.load(os.path.join(ROOT, "tests", "golden", "migrator_lut.npz"))
+    ox, oy, dx, dy, nil, nxl, dt, tmin, v, A, ang, nt, gdt = g["grid"]
+    il = np.arange(int(nil))[:, None]
+    xl = np.arange(int(nxl))[None, :]
+    cx = (ox + il * dx + 0 * xl).ravel()
+    cy = (oy + 0 * il + xl * dy).ravel()
+    t_ms = (np.arange(int(nt)) * gdt).astype(np.float32).astype(np.float64) * 1000.0
+    for name in ("constant", "gradient"):
+        v0, k = float(g[f"v0_{name}"]), float(g[f"gradient_{name}"])
+        img, fold = O.migrate_fp64(g["traces"], g["source_x"], g["source_y"], g["receiver_x"],
+                                   g["receiver_y"], cx, cy, t_ms, v0, float(dt), 0.0, float(A),
+                                   float(ang), weight="spreading", clamp="migrator",
+                                   ray_gradient=k)
+        ref = g[f"image_{name}"].reshape(int(nt), -1)
+        assert np.linalg.norm(img - ref) <= 5e-5 * np.linalg.norm(ref), name
+        assert np.array_equal(fold, g[f"fold_{name}"].reshape(int(nt), -1))
