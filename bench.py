@@ -9,7 +9,7 @@ aperture, 60 deg angle.  Synthetic, seeded.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|bf16|f16]
                   [--antialias] [--utm]
   python bench.py --impl reference ...   (CPU port of the reference kernel)
-  python bench.py --config batched | lsq | velocity
+  python bench.py --config batched | lsq | velocity | time_rms
 
 ``--antialias --utm --storage bf16|f16`` is the anti-aliased workload with
 traces stored in 16 bits and world coordinates offset by a UTM origin.  Every
@@ -691,6 +691,159 @@ def bench_velocity(args):
     }), flush=True)
 
 
+def bench_time_rms(args):
+    """The time-domain RMS operator (MigrationEngine.migrate_bin_time_domain_rms)
+    on the 3D survey's geometry: N traces with midpoints over 5 x 5 km, offsets
+    up to 3 km, V_rms with a linear gradient, the 200 x 200 x 1000 output grid
+    at 25 m, aperture 1000 m, 60 deg, time-dependent aperture, the reference's
+    default tiles (100 points) and trace cap (5000 per tile).
+    value = evaluated (output point, trace, input sample) triples per second of
+    pstm_time_rms_migrate with inputs resident (points within the aperture
+    only: the kernel skips the others before the sample loop); roofline = 8
+    MUFU operations per triple (five IEEE divisions, three IEEE square roots);
+    e2e = the whole engine call from host arrays; cpu_baseline = the float32
+    oracle on one tile."""
+    from seisproc_b200 import _lib
+    from seisproc_b200 import time_domain as TD
+    from seisproc_b200.engine import MigrationEngine
+    from seisproc_b200.velocity import VelocityModel
+    sys.path.insert(0, ROOT)
+    from oracle import time_domain as otd
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    L = _lib.lib()
+    n_tr, n_s, n = args.traces, args.samples, args.grid
+    sp, dt, A, theta = 25.0, 4.0, 1000.0, 60.0
+    rs = np.random.RandomState(2025)
+    mx, my = rs.uniform(0, 5000, n_tr), rs.uniform(0, 5000, n_tr)
+    off, phi = rs.uniform(0, 3000, n_tr), rs.uniform(0, 2 * np.pi, n_tr)
+    sx = (mx - 0.5 * off * np.cos(phi)).astype(np.float32)
+    sy = (my - 0.5 * off * np.sin(phi)).astype(np.float32)
+    rx = (mx + 0.5 * off * np.cos(phi)).astype(np.float32)
+    ry = (my + 0.5 * off * np.sin(phi)).astype(np.float32)
+    tr = rs.standard_normal((n_s, n_tr)).astype(np.float32)
+    vm = VelocityModel("gradient", 1500.0, gradient=0.6)
+    grid = dict(origin_x=12.5, origin_y=12.5, il_spacing=sp, xl_spacing=sp, azimuth_deg=0.0,
+                n_il=n, n_xl=n, dt_ms=dt, t_min_ms=0.0, n_times=n_s)
+    # resident inputs, built once as the engine builds them
+    f32 = torch.float32
+    d_tr = torch.from_numpy(tr).to(dev)
+    g = [torch.from_numpy(a).to(dev) for a in (sx, sy, rx, ry)]
+    il = torch.arange(n, device=dev, dtype=f32) * sp
+    xl_g, il_g = torch.meshgrid(il, il, indexing="xy")
+    ox = (12.5 + il_g.flatten()).contiguous()
+    oy = (12.5 + xl_g.flatten()).contiguous()
+    t_axis = torch.arange(n_s, device=dev, dtype=f32) * dt
+    tile = TD.effective_tile_size(100, 5000, 200)
+    mid_x, mid_y, _, _ = TD.trace_geometry(*g, 12.5, 12.5, sp, sp, 0.0, n, n)
+    p_tile, p_trace = TD.tile_pairs(ox, oy, mid_x, mid_y, tile, A, 5000)
+    # algorithmic work: (pair, point) with h < A, times the input samples
+    evals = 0
+    for a in range(0, p_tile.numel(), 1 << 18):
+        pt, pj = p_tile[a:a + (1 << 18)], p_trace[a:a + (1 << 18)]
+        pts = pt[:, None] * tile + torch.arange(tile, device=dev)[None, :]
+        ok = pts < n * n
+        pts = pts.clamp(max=n * n - 1)
+        h = torch.sqrt((ox[pts] - mid_x[pj][:, None]) ** 2 + (oy[pts] - mid_y[pj][:, None]) ** 2)
+        evals += int(((h < A) & ok).sum())
+    evals *= n_s
+
+    def run():
+        return TD.migrate_kirchhoff_time_domain_rms(
+            d_tr, *g, ox, oy, t_axis, vm, dt, 0.0, A, theta, n, n, 12.5, 12.5, sp, sp, 0.0)
+
+    for _ in range(args.warmup):
+        run()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    # kernel-only times: the pair list and V_rms table are rebuilt per call,
+    # so the kernel is timed by its own events inside a patched launcher
+    k_ms = []
+    orig = L.pstm_time_rms_migrate
+
+    class Timed:
+        def __call__(self, *a):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            st = orig(*a)
+            e.record()
+            k_ms.append((s, e))
+            return st
+    l0 = L.pstm_launch_count()
+    _lib._lib.pstm_time_rms_migrate = Timed()
+    try:
+        with ClockSampler(0) as clk:
+            for a, b in ev:
+                a.record()
+                run()
+                b.record()
+            torch.cuda.synchronize()
+    finally:
+        _lib._lib.pstm_time_rms_migrate = orig
+    launches = L.pstm_launch_count() - l0
+    call_ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+    kern_ms = statistics.median(s.elapsed_time(e) for s, e in k_ms)
+    # e2e: the engine call from host arrays (H2D, plan, kernel, D2H)
+    eng = MigrationEngine()
+    e2e_ms = []
+    for _ in range(max(2, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        img, fold = eng.migrate_bin_time_domain_rms(
+            tr, sx, sy, rx, ry, velocity_model=vm, max_aperture_m=A, max_angle_deg=theta,
+            normalize=False, **grid)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e = statistics.median(e2e_ms)
+    # CPU: the float32 oracle on the first tile with pairs (500 of its traces),
+    # scaled per evaluation
+    cpu = None
+    if not args.no_cpu:
+        t_sel = int(p_tile[0])
+        sel = p_trace[p_tile == t_sel].cpu().numpy()[:500]
+        pts = np.arange(t_sel * tile, min((t_sel + 1) * tile, n * n))
+        oxn, oyn = ox.cpu().numpy(), oy.cpu().numpy()
+        mxn, myn = mid_x.cpu().numpy(), mid_y.cpu().numpy()
+        hh = np.sqrt((oxn[pts, None] - mxn[None, sel]) ** 2 + (oyn[pts, None] - myn[None, sel]) ** 2)
+        ev_cpu = int((hh < A).sum()) * n_s
+        v_in = vm.rms_velocity_at_time(t_axis.cpu()).numpy()
+        t0 = time.perf_counter()
+        tiles_one = [(pts[0], pts[-1] + 1, sel)]
+        orig_lists = otd.tile_trace_lists
+        otd.tile_trace_lists = lambda *a, **k: tiles_one
+        try:
+            otd.time_domain_rms_f32(tr, sx, sy, rx, ry, v_in, 12.5, 12.5, sp, sp, 0.0, n, n, dt,
+                                    0.0, n_s, A, theta)
+        finally:
+            otd.tile_trace_lists = orig_lists
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": ev_cpu / cpu_s / 1e9, "unit": "Gevals/s", "cores": 1, "kind": "port",
+               "sample": f"one tile: {pts.size} points x {sel.size} of its traces x {n_s} samples, "
+                         "float32 numpy oracle"}
+    pk = peaks()
+    mufu_peak = 148 * 16 * pk["sm_max_mhz"] * 1e6 / 8 / 1e9  # Gevals/s
+    val = evals / (kern_ms * 1e-3) / 1e9
+    print(json.dumps({
+        "metric": "time-domain RMS scatter Gevals/s", "value": val, "unit": "Gevals/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": kern_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"time-domain RMS operator, {n_tr} traces x {n_s} samples, "
+                               f"{n}x{n}x{n_s} output grid, aperture {A:.0f} m, {theta:.0f} deg, "
+                               "tiles of 100 points, 5000-trace cap",
+                   "pairs": int(p_tile.numel()), "evals": evals,
+                   "l2": "inputs (traces 2 GB) larger than L2"},
+        "call_ms": call_ms,
+        "roofline": {"bound": "mufu", "achieved": val, "peak": mufu_peak, "unit": "Gevals/s",
+                     "frac": val / mufu_peak, "traffic": None,
+                     "mufu_per_eval": 8, "peak_source": pk["source"]},
+        "e2e": {"value": evals / (e2e * 1e-3) / 1e9, "unit": "Gevals/s",
+                "h2d_bytes_per_step": int(tr.nbytes + 16 * n_tr),
+                "d2h_bytes_per_step": int(2 * 4 * n * n * n_s), "ms_per_step": e2e},
+        "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk.summary(),
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -715,7 +868,8 @@ def main():
     ap.add_argument("--lsq-traces", type=int, default=120_000)
     ap.add_argument("--cg-iters", type=int, default=10)
     ap.add_argument("--fd-directions", type=int, default=20)
-    ap.add_argument("--config", default="3d", choices=["3d", "batched", "lsq", "velocity"])
+    ap.add_argument("--config", default="3d",
+                    choices=["3d", "batched", "lsq", "velocity", "time_rms"])
     args = ap.parse_args()
     if args.config == "batched" and args.impl == "ours":
         return bench_batched(args)
@@ -723,6 +877,8 @@ def main():
         return bench_lsq(args)
     if args.config == "velocity" and args.impl == "ours":
         return bench_velocity(args)
+    if args.config == "time_rms" and args.impl == "ours":
+        return bench_time_rms(args)
     if args.impl == "reference":
         bench_reference(args)
     else:

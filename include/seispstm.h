@@ -257,6 +257,54 @@ pstm_status pstm_velocity_grid(const float* model, int32_t nz, int32_t nx, int32
                                const int32_t* ix, const double* wx, const int32_t* iy,
                                const double* wy, int64_t n_cols, float* out, void* stream);
 
+/* ---- time-domain RMS operator (compatibility entry) -------------------- */
+
+/* Sizes and parameters of pstm_time_rms_migrate.  Input sample i is at time
+ * i * dt_ms (input traces start at t = 0); output time k at t_min_ms + k * dt_ms. */
+typedef struct pstm_time_rms_params {
+  int64_t n_samples;              /* input samples per trace, <= 2^24 */
+  int64_t n_traces;
+  int64_t n_points;               /* output points n_il * n_xl, il-major */
+  int32_t n_times;                /* output times */
+  int32_t tile;                   /* output points per tile (consecutive) */
+  double dt_ms, t_min_ms;
+  double max_aperture_m, max_angle_deg;
+  int32_t time_dependent_aperture;
+} pstm_time_rms_params;
+
+/* The reference's time-domain RMS operator, migrate_kirchhoff_time_domain_rms
+ * (processors/migration/kirchhoff_kernel.py:1313-1783, behind
+ * MigrationEngine.migrate_bin_time_domain_rms, migration_engine.py:633-802) --
+ * a different operator from pstm_migrate's Kirchhoff summation.  For each
+ * (tile, trace) pair every input sample maps to
+ * t_out = sqrt(t_in^2 + 4 h_eff^2 / V_rms(t_in)^2) for every output point of
+ * the tile (h = point-to-midpoint distance, h_eff^2 = h^2 + half-offset^2),
+ * masked by output range, aperture and angle, weighted by z / (r^3 + 1e-10),
+ * and added at the truncated output index into the TRACE's own midpoint
+ * column, with fold counted alongside.  The index arithmetic is the
+ * reference's float32 sequence, so every contribution lands where the
+ * reference puts it.
+ *
+ * Device pointers: traces (n_samples, n_traces) float32 sample-major;
+ * mid_x/mid_y/half_offset_sq per trace; out_x/out_y per output point; v_rms
+ * per input sample.  The caller forms the pairs the reference's per-tile
+ * trace selection yields (midpoint within aperture + tile radius + 100 m of
+ * the tile centre, the nearest max_traces_per_tile kept), sorted by the
+ * trace's column: pair q is (pair_trace[q], pair_tile[q]), and segment g,
+ * pairs seg_off[g] .. seg_off[g + 1] - 1 (n_segments + 1 offsets), all have
+ * column seg_col[g] (il * n_xl + xl), one segment per column.  Pairs or
+ * segments out of range are skipped.  image and fold, (n_times, n_points)
+ * float32, are overwritten.  Requires 2 n_times + 3 n_samples <= 58112 (the
+ * per-column sums and the staged trace live in shared memory). */
+pstm_status pstm_time_rms_migrate(const pstm_time_rms_params* params, const float* traces,
+                                  const float* mid_x, const float* mid_y,
+                                  const float* half_offset_sq, const float* out_x,
+                                  const float* out_y, const float* v_rms,
+                                  const int32_t* pair_trace, const int32_t* pair_tile,
+                                  int64_t n_pairs, const int64_t* seg_off,
+                                  const int32_t* seg_col, int64_t n_segments, float* image,
+                                  float* fold, void* stream);
+
 /* ---- batched migration: many plans in one persistent launch ------------- */
 typedef struct pstm_batch pstm_batch;
 

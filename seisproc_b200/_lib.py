@@ -52,6 +52,14 @@ class PlanStats(C.Structure):
                 ("t_window", C.c_int32), ("variant", C.c_int32)]
 
 
+class TimeRmsParams(C.Structure):
+    _fields_ = [("n_samples", C.c_int64), ("n_traces", C.c_int64), ("n_points", C.c_int64),
+                ("n_times", C.c_int32), ("tile", C.c_int32),
+                ("dt_ms", C.c_double), ("t_min_ms", C.c_double),
+                ("max_aperture_m", C.c_double), ("max_angle_deg", C.c_double),
+                ("time_dependent_aperture", C.c_int32)]
+
+
 class PSTMError(RuntimeError):
     """A non-OK status from libseispstm."""
 
@@ -97,6 +105,8 @@ _SIGNATURES = {
                                      _P, _P, _P, _P, C.c_int64, _P, _P]),
     "pstm_migrate_noalloc": (C.c_int, [C.POINTER(Grid), C.POINTER(Params), C.POINTER(Geometry),
                                        _P, _P, C.c_int64, C.c_int64, _P, _P, _P]),
+    "pstm_time_rms_migrate": (C.c_int, [C.POINTER(TimeRmsParams), _P, _P, _P, _P, _P, _P, _P,
+                                        _P, _P, C.c_int64, _P, _P, C.c_int64, _P, _P, _P]),
 }
 
 

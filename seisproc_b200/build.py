@@ -29,6 +29,7 @@ SOURCES = [
     "pstm_noalloc.cu",
     "pstm_batch.cu",
     "pstm_velocity.cu",
+    "pstm_time_domain.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from .kernel_backend import require_cuda
-from .kirchhoff import PSTMPlan
+from .kirchhoff import PSTMPlan, normalize_by_fold
 from . import models as _models
 from . import velocity as _velocity
 from .velocity_io import velocity_grid
@@ -368,5 +368,73 @@ class MigrationEngine:
     def migrate_bin_time_domain(self, *a, **k):
         self._not_this_operator("migrate_bin_time_domain")
 
-    def migrate_bin_time_domain_rms(self, *a, **k):
-        self._not_this_operator("migrate_bin_time_domain_rms")
+    def migrate_bin_time_domain_rms(
+        self,
+        traces: np.ndarray,
+        source_x: np.ndarray,
+        source_y: np.ndarray,
+        receiver_x: np.ndarray,
+        receiver_y: np.ndarray,
+        origin_x: float,
+        origin_y: float,
+        il_spacing: float,
+        xl_spacing: float,
+        azimuth_deg: float,
+        n_il: int,
+        n_xl: int,
+        dt_ms: float,
+        t_min_ms: float,
+        n_times: int,
+        velocity_model,
+        max_aperture_m: float = 5000.0,
+        max_angle_deg: float = 60.0,
+        tile_size: int = 100,
+        sample_batch_size: int = 200,
+        max_traces_per_tile: int = 5000,
+        normalize: bool = True,
+        min_fold: int = 1,
+        progress_callback: Optional[Callable[[float, str], None]] = None,
+        enable_profiling: bool = False,
+        use_time_dependent_aperture: bool = True,
+    ) -> Tuple[np.ndarray, np.ndarray]:
+        """The reference's time-domain RMS operator (migration_engine.py:633-802):
+        each trace's samples moved by t_out = sqrt(t_in^2 + 4 h_eff^2 / V_rms^2)
+        into its own midpoint column, on the ``pstm_time_rms_migrate`` kernel.
+        A different operator from ``migrate_bin_full``; same arguments and
+        results as the reference, (image, fold) (n_times, n_il, n_xl) float32."""
+        from .time_domain import migrate_kirchhoff_time_domain_rms
+        dev = self.device
+        f32 = torch.float32
+        if progress_callback:
+            progress_callback(0.0, "Preparing data...")
+        with torch.cuda.device(dev):
+            tr = torch.from_numpy(np.ascontiguousarray(traces, np.float32)).to(dev)
+            sx, sy, rx, ry = (torch.from_numpy(np.asarray(a, np.float32)).to(dev)
+                              for a in (source_x, source_y, receiver_x, receiver_y))
+            # output grid as migration_engine.py:727-737 builds it
+            cos_az = np.cos(np.radians(azimuth_deg))
+            sin_az = np.sin(np.radians(azimuth_deg))
+            il = torch.arange(n_il, device=dev, dtype=f32) * il_spacing
+            xl = torch.arange(n_xl, device=dev, dtype=f32) * xl_spacing
+            xl_g, il_g = torch.meshgrid(xl, il, indexing="xy")
+            out_x = origin_x + il_g.flatten() * cos_az - xl_g.flatten() * sin_az
+            out_y = origin_y + il_g.flatten() * sin_az + xl_g.flatten() * cos_az
+            t_axis = torch.arange(n_times, device=dev, dtype=f32) * dt_ms + t_min_ms
+
+            def kernel_progress(pct: float, msg: str):
+                if progress_callback:
+                    progress_callback(0.1 + pct * 0.8, msg)
+
+            image, fold = migrate_kirchhoff_time_domain_rms(
+                tr, sx, sy, rx, ry, out_x, out_y, t_axis, velocity_model, dt_ms, t_min_ms,
+                max_aperture_m, max_angle_deg, n_il, n_xl, origin_x, origin_y, il_spacing,
+                xl_spacing, azimuth_deg, tile_size=tile_size,
+                sample_batch_size=sample_batch_size, max_traces_per_tile=max_traces_per_tile,
+                progress_callback=kernel_progress, enable_profiling=enable_profiling,
+                use_time_dependent_aperture=use_time_dependent_aperture)
+            if normalize:
+                image = normalize_by_fold(image, fold, min_fold)
+            out = image.cpu().numpy(), fold.cpu().numpy()
+        if progress_callback:
+            progress_callback(1.0, "Complete")
+        return out

@@ -13,6 +13,7 @@ from dataclasses import dataclass
 from typing import Optional
 
 import numpy as np
+import torch
 
 
 @dataclass
@@ -38,7 +39,12 @@ class VelocityModel:
         return np.interp(z, self.z_axis, self.velocity_array)
 
     def rms_velocity_at_time(self, t_ms):
-        """V_rms at two-way time t (ms); numpy arrays in, float32 arrays out."""
+        """V_rms at two-way time t (ms); numpy arrays in, float32 arrays out.
+        A float32 torch tensor gives a float32 tensor on its device, with the
+        gradient formula evaluated in float32 in the reference's order
+        (velocity_model.py:155-175), as the reference's tensor branch does."""
+        if isinstance(t_ms, torch.Tensor):
+            return self._rms_velocity_tensor(t_ms)
         scalar = np.ndim(t_ms) == 0
         t = np.asarray(t_ms, np.float64)
         if self.velocity_type == "constant" or (self.velocity_type == "gradient"
@@ -56,6 +62,23 @@ class VelocityModel:
             tt, vv = self._table
             out = np.interp(t, tt, vv).astype(np.float32)
         return float(out) if scalar else out
+
+    def _rms_velocity_tensor(self, t: torch.Tensor) -> torch.Tensor:
+        if self.velocity_type == "constant" or (self.velocity_type == "gradient"
+                                                and abs(self.gradient) < 1e-10):
+            return torch.full_like(t, self.v0)
+        if self.velocity_type == "gradient":
+            v0, k = self.v0, self.gradient
+            # divisors as tensors: a CUDA tensor divided by a Python number is
+            # multiplied by the float32 reciprocal, which rounds differently
+            tw = t / torch.tensor(2000.0, dtype=t.dtype, device=t.device)
+            z = torch.clamp(v0 * tw + 0.5 * k * v0 * tw * tw, min=0)
+            vs = v0 * v0 + v0 * k * z + (k * k * z * z) / torch.tensor(3.0, dtype=t.dtype,
+                                                                         device=t.device)
+            v = torch.sqrt(torch.clamp(vs, min=v0 * v0 * 0.5))
+            return torch.where(t < 1.0, torch.full_like(v, v0), v)
+        out = self.rms_velocity_at_time(t.detach().cpu().numpy())
+        return torch.from_numpy(np.asarray(out, np.float32)).to(t.device)
 
     def _build_table(self):
         z = np.asarray(self.z_axis, np.float64)

@@ -1,0 +1,130 @@
+"""Time-domain RMS operator, CPU side: the oracle against golden vectors from
+the reference's migrate_bin_time_domain_rms, the host logic (midpoint columns,
+tile trace lists, V_rms table) against the oracle, and the C entry point's
+argument validation (no device work)."""
+import ctypes as C
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden, rel_l2
+from oracle import time_domain as otd
+
+
+def _cases():
+    g = load_golden("time_domain_rms")
+    return g, json.loads(str(g["cases_json"]))
+
+
+def _velocity_model(g, c):
+    from seisproc_b200.velocity import VelocityModel
+    kind, v0, k = c["vel"]
+    if kind == "file":
+        return VelocityModel("file", float(g["file_v"][0]), velocity_array=g["file_v"],
+                             z_axis=g["file_z"])
+    return VelocityModel(kind, v0, gradient=k)
+
+
+def _oracle(g, n, c, v_in=None):
+    img, fold = otd.time_domain_rms_f32(
+        g[n + "_traces"], g[n + "_sx"], g[n + "_sy"], g[n + "_rx"], g[n + "_ry"],
+        g[n + "_v_in"] if v_in is None else v_in, c["origin"][0], c["origin"][1],
+        c["il_spacing"], c["xl_spacing"], c["azimuth_deg"], c["n_il"], c["n_xl"], c["dt_ms"],
+        c["t_min_ms"], c["n_times"], c["max_aperture_m"], c["max_angle_deg"], c["tile_size"],
+        200, c["max_traces_per_tile"], c["tda"])
+    if c["normalize"]:
+        m = fold >= c["min_fold"]
+        img = img.copy()
+        img[m] = img[m] / fold[m]
+    return img, fold
+
+
+@pytest.mark.parametrize("name", ["c0", "c1", "c2"])
+def test_oracle_matches_reference_golden(name):
+    g, cases = _cases()
+    img, fold = _oracle(g, name, cases[name])
+    np.testing.assert_array_equal(fold, g[name + "_fold"])
+    assert rel_l2(img, g[name + "_image"]) < 1e-6
+    assert g[name + "_fold"].sum() > 1000  # the case has contributions
+
+
+@pytest.mark.parametrize("name", ["c0", "c1", "c2"])
+def test_velocity_table_matches_reference(name):
+    """The engine VelocityModel's tensor branch gives the reference's float32
+    V_rms at the input times, bit for bit."""
+    g, cases = _cases()
+    c = cases[name]
+    t_in = 0.0 + torch.arange(c["n_s"], dtype=torch.float32) * c["dt_ms"]
+    v = _velocity_model(g, c).rms_velocity_at_time(t_in)
+    np.testing.assert_array_equal(v.numpy(), g[name + "_v_in"])
+    if c["vel"][0] != "file":
+        np.testing.assert_array_equal(
+            otd.rms_velocity_torch_order_f32(c["vel"][0], c["vel"][1], c["vel"][2],
+                                             t_in.numpy()), g[name + "_v_in"])
+
+
+@pytest.mark.parametrize("name", ["c0", "c1", "c2"])
+def test_host_pairs_and_columns_match_oracle(name):
+    from seisproc_b200 import time_domain as td
+    g, cases = _cases()
+    c = cases[name]
+    t = {k: torch.from_numpy(g[f"{name}_{k}"]) for k in ("sx", "sy", "rx", "ry")}
+    mid_x, mid_y, hoff, col = td.trace_geometry(t["sx"], t["sy"], t["rx"], t["ry"],
+                                                c["origin"][0], c["origin"][1],
+                                                c["il_spacing"], c["xl_spacing"],
+                                                c["azimuth_deg"], c["n_il"], c["n_xl"])
+    mx = (g[name + "_sx"] + g[name + "_rx"]) / np.float32(2)
+    my = (g[name + "_sy"] + g[name + "_ry"]) / np.float32(2)
+    np.testing.assert_array_equal(mid_x.numpy(), mx)
+    il, xl = otd.trace_columns_f32(mx, my, c["origin"][0], c["origin"][1], c["il_spacing"],
+                                   c["xl_spacing"], c["azimuth_deg"], c["n_il"], c["n_xl"])
+    np.testing.assert_array_equal(col.numpy(), il * c["n_xl"] + xl)
+    ox, oy = otd.output_grid_f32(c["origin"][0], c["origin"][1], c["il_spacing"],
+                                 c["xl_spacing"], c["azimuth_deg"], c["n_il"], c["n_xl"])
+    tile = td.effective_tile_size(c["tile_size"], c["max_traces_per_tile"], 200)
+    assert tile == otd.effective_tile_size(c["tile_size"], c["max_traces_per_tile"], 200)
+    p_tile, p_trace = td.tile_pairs(torch.from_numpy(ox), torch.from_numpy(oy), mid_x, mid_y,
+                                    tile, c["max_aperture_m"], c["max_traces_per_tile"],
+                                    elements=4096)
+    want = {(i, int(j)) for i, (_, _, sel) in enumerate(
+        otd.tile_trace_lists(ox, oy, mx, my, tile, c["max_aperture_m"],
+                             c["max_traces_per_tile"])) for j in sel}
+    got = set(zip(p_tile.tolist(), p_trace.tolist()))
+    assert got == want
+    if c["max_traces_per_tile"] < 1000:  # the cap bites in this case
+        counts = np.bincount(p_tile.numpy())
+        assert counts.max() == c["max_traces_per_tile"]
+
+
+def test_effective_tile_size_follows_memory_bound():
+    from seisproc_b200.time_domain import effective_tile_size
+    assert effective_tile_size(100, 5000, 200) == 100
+    assert effective_tile_size(1000, 5000, 200) == 322
+    assert effective_tile_size(1000, 10 ** 6, 400) == 50
+
+
+def test_entry_point_rejects_bad_arguments_without_device():
+    from seisproc_b200 import _lib
+    L = _lib.lib()
+    fn = L.pstm_time_rms_migrate
+    z = [None] * 9
+    assert fn(None, *z[:9], 0, None, None, 0, None, None, None) == _lib.PSTM_EINVAL
+    assert "params" in _lib.last_error()
+    buf = (C.c_float * 4)()
+    good = dict(n_samples=10, n_traces=1, n_points=1, n_times=2, tile=1, dt_ms=4.0,
+                t_min_ms=0.0, max_aperture_m=100.0, max_angle_deg=60.0,
+                time_dependent_aperture=1)
+    for bad in (dict(n_samples=0), dict(n_times=0), dict(tile=0), dict(dt_ms=0.0),
+                dict(n_points=0), dict(max_angle_deg=float("nan")), dict(n_times=30000)):
+        p = _lib.TimeRmsParams(**{**good, **bad})
+        st = fn(C.byref(p), *z[:9], 0, None, None, 0, C.cast(buf, C.c_void_p),
+                C.cast(buf, C.c_void_p), None)
+        assert st == _lib.PSTM_EINVAL, bad
+    p = _lib.TimeRmsParams(**good)
+    assert fn(C.byref(p), *z[:9], 0, None, None, 0, None, None, None) == _lib.PSTM_EINVAL
+    # segments to process but NULL inputs
+    assert fn(C.byref(p), *z[:9], 1, None, None, 1, C.cast(buf, C.c_void_p),
+              C.cast(buf, C.c_void_p), None) == _lib.PSTM_EINVAL
+    assert "NULL input" in _lib.last_error()
