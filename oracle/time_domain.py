@@ -85,12 +85,14 @@ def time_domain_rms_f32(traces, source_x, source_y, receiver_x, receiver_y, v_rm
                         origin_x, origin_y, il_spacing, xl_spacing, azimuth_deg, n_il, n_xl,
                         dt_ms, t_min_ms, n_times, max_aperture_m, max_angle_deg,
                         tile_size=100, sample_batch_size=200, max_traces_per_tile=5000,
-                        use_time_dependent_aperture=True, batch=64):
+                        use_time_dependent_aperture=True, batch=64, tiles=None):
     """(image, fold) as float64 sums of the reference's float32 terms.
 
     ``traces`` (n_samples, n_traces) float32; ``v_rms_in`` the float32 V_rms at
     each INPUT time i * dt_ms (input traces start at t = 0,
-    kirchhoff_kernel.py:1474-1484)."""
+    kirchhoff_kernel.py:1474-1484).  ``tiles``, a list of (first point, end
+    point, trace indices), restricts the sum to those tiles (default: every
+    tile, with the reference's trace lists)."""
     traces = np.asarray(traces, f32)
     n_s, n_tr = traces.shape
     sx, sy = np.asarray(source_x, f32), np.asarray(source_y, f32)
@@ -116,8 +118,10 @@ def time_domain_rms_f32(traces, source_x, source_y, receiver_x, receiver_y, v_rm
     image = np.zeros(n_times * n_cols, np.float64)
     fold = np.zeros(n_times * n_cols, np.float64)
 
-    for p0, p1, sel in tile_trace_lists(ox, oy, mid_x, mid_y, tile, max_aperture_m,
-                                        max_traces_per_tile):
+    if tiles is None:
+        tiles = tile_trace_lists(ox, oy, mid_x, mid_y, tile, max_aperture_m,
+                                 max_traces_per_tile)
+    for p0, p1, sel in tiles:
         if sel.size == 0:
             continue
         dx = ox[p0:p1, None] - mid_x[None, sel]

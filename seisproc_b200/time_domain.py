@@ -117,6 +117,48 @@ def tile_pairs(output_x: torch.Tensor, output_y: torch.Tensor, mid_x: torch.Tens
     return torch.cat(tiles), torch.cat(traces)
 
 
+def column_pairs(output_x: torch.Tensor, output_y: torch.Tensor, mid_x: torch.Tensor,
+                 mid_y: torch.Tensor, col: torch.Tensor, tile: int, max_aperture_m: float,
+                 max_traces_per_tile: int):
+    """The (tile, trace) pairs in the form ``pstm_time_rms_migrate`` takes them:
+    sorted by the trace's midpoint column (stable, so tile order is kept within
+    a column), as (pair_trace int32, pair_tile int32, seg_off int64 with one
+    more entry than there are columns with pairs, seg_col int32)."""
+    p_tile, p_trace = tile_pairs(output_x, output_y, mid_x, mid_y, tile, max_aperture_m,
+                                 max_traces_per_tile)
+    key, order = torch.sort(col[p_trace], stable=True)
+    pair_trace = p_trace[order].to(torch.int32).contiguous()
+    pair_tile = p_tile[order].to(torch.int32).contiguous()
+    seg_col, counts = torch.unique_consecutive(key, return_counts=True)
+    seg_off = torch.zeros(seg_col.numel() + 1, dtype=torch.int64, device=key.device)
+    torch.cumsum(counts, 0, out=seg_off[1:])
+    return pair_trace, pair_tile, seg_off, seg_col.to(torch.int32).contiguous()
+
+
+def launch_time_rms(traces: torch.Tensor, mid_x: torch.Tensor, mid_y: torch.Tensor,
+                    hoff_sq: torch.Tensor, output_x: torch.Tensor, output_y: torch.Tensor,
+                    v_rms: torch.Tensor, pairs, tile: int, dt_ms: float, t_min_ms: float,
+                    max_aperture_m: float, max_angle_deg: float,
+                    use_time_dependent_aperture: bool, image: torch.Tensor,
+                    fold: torch.Tensor) -> None:
+    """One ``pstm_time_rms_migrate`` launch on the current stream: ``traces``
+    (n_samples, n_traces) float32, the per-trace and per-point float32 arrays,
+    V_rms per input sample, ``pairs`` from ``column_pairs``; image and fold
+    (n_times, n_points) float32 contiguous, overwritten."""
+    n_s, n_tr = traces.shape
+    pair_trace, pair_tile, seg_off, seg_col = pairs
+    p = _lib.TimeRmsParams(n_samples=n_s, n_traces=n_tr, n_points=output_x.numel(),
+                           n_times=image.shape[0], tile=tile, dt_ms=float(dt_ms),
+                           t_min_ms=float(t_min_ms), max_aperture_m=float(max_aperture_m),
+                           max_angle_deg=float(max_angle_deg),
+                           time_dependent_aperture=1 if use_time_dependent_aperture else 0)
+    args = [a.contiguous() for a in (traces, mid_x, mid_y, hoff_sq, output_x, output_y, v_rms)]
+    _lib.check(_lib.lib().pstm_time_rms_migrate(
+        C.byref(p), *(_ptr(a) for a in args), _ptr(pair_trace), _ptr(pair_tile),
+        int(pair_trace.numel()), _ptr(seg_off), _ptr(seg_col), int(seg_col.numel()),
+        _ptr(image), _ptr(fold), _stream_handle()))
+
+
 def migrate_kirchhoff_time_domain_rms(
     traces: torch.Tensor,
     source_x: torch.Tensor,
@@ -179,29 +221,13 @@ def migrate_kirchhoff_time_domain_rms(
     v = (v if isinstance(v, torch.Tensor) else torch.as_tensor(np.asarray(v))).to(dev, f32)
     v = v.expand(n_s).contiguous()
 
-    p_tile, p_trace = tile_pairs(ox, oy, mid_x, mid_y, tile, max_aperture_m,
-                                 max_traces_per_tile)
-    key, order = torch.sort(col[p_trace], stable=True)
-    pair_trace = p_trace[order].to(torch.int32).contiguous()
-    pair_tile = p_tile[order].to(torch.int32).contiguous()
-    seg_col, counts = torch.unique_consecutive(key, return_counts=True)
-    seg_off = torch.zeros(seg_col.numel() + 1, dtype=torch.int64, device=dev)
-    torch.cumsum(counts, 0, out=seg_off[1:])
-    seg_col = seg_col.to(torch.int32).contiguous()
-
+    pairs = column_pairs(ox, oy, mid_x, mid_y, col, tile, max_aperture_m, max_traces_per_tile)
     image = torch.empty((n_times, n_il, n_xl), dtype=f32, device=dev)
     fold = torch.empty_like(image)
-    p = _lib.TimeRmsParams(n_samples=n_s, n_traces=n_tr, n_points=n_out, n_times=n_times,
-                           tile=tile, dt_ms=float(dt_ms), t_min_ms=float(t_min_ms),
-                           max_aperture_m=float(max_aperture_m),
-                           max_angle_deg=float(max_angle_deg),
-                           time_dependent_aperture=1 if use_time_dependent_aperture else 0)
-    mx, my, ho = mid_x.contiguous(), mid_y.contiguous(), hoff_sq.contiguous()
     with torch.cuda.device(dev):
-        _lib.check(_lib.lib().pstm_time_rms_migrate(
-            C.byref(p), _ptr(tr), _ptr(mx), _ptr(my), _ptr(ho), _ptr(ox), _ptr(oy), _ptr(v),
-            _ptr(pair_trace), _ptr(pair_tile), int(pair_trace.numel()), _ptr(seg_off),
-            _ptr(seg_col), int(seg_col.numel()), _ptr(image), _ptr(fold), _stream_handle()))
+        launch_time_rms(tr, mid_x, mid_y, hoff_sq, ox, oy, v, pairs, tile, dt_ms, t_min_ms,
+                        max_aperture_m, max_angle_deg, use_time_dependent_aperture, image, fold)
+    pair_trace, seg_col = pairs[0], pairs[3]
     if enable_profiling:
         torch.cuda.synchronize(dev)
         logger.info("time-domain (RMS): %d tiles of %d points, %d (tile, trace) pairs, "

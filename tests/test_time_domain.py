@@ -128,3 +128,35 @@ def test_entry_point_rejects_bad_arguments_without_device():
     assert fn(C.byref(p), *z[:9], 1, None, None, 1, C.cast(buf, C.c_void_p),
               C.cast(buf, C.c_void_p), None) == _lib.PSTM_EINVAL
     assert "NULL input" in _lib.last_error()
+
+
+@pytest.mark.parametrize("name", ["c0", "c1"])
+def test_column_pairs_sorted_by_midpoint_column(name):
+    """The pair list the kernel takes: every selected (tile, trace) pair once,
+    grouped by the trace's midpoint column, one segment per column."""
+    from seisproc_b200 import time_domain as td
+    g, cases = _cases()
+    c = cases[name]
+    t = {k: torch.from_numpy(g[f"{name}_{k}"]) for k in ("sx", "sy", "rx", "ry")}
+    mid_x, mid_y, _, col = td.trace_geometry(t["sx"], t["sy"], t["rx"], t["ry"],
+                                             c["origin"][0], c["origin"][1], c["il_spacing"],
+                                             c["xl_spacing"], c["azimuth_deg"], c["n_il"],
+                                             c["n_xl"])
+    ox, oy = (torch.from_numpy(a) for a in otd.output_grid_f32(
+        c["origin"][0], c["origin"][1], c["il_spacing"], c["xl_spacing"], c["azimuth_deg"],
+        c["n_il"], c["n_xl"]))
+    tile = td.effective_tile_size(c["tile_size"], c["max_traces_per_tile"], 200)
+    args = (ox, oy, mid_x, mid_y)
+    p_tile, p_trace = td.tile_pairs(*args, tile, c["max_aperture_m"], c["max_traces_per_tile"])
+    pair_trace, pair_tile, seg_off, seg_col = td.column_pairs(
+        *args, col, tile, c["max_aperture_m"], c["max_traces_per_tile"])
+    assert pair_trace.dtype == torch.int32 and seg_off.dtype == torch.int64
+    assert set(zip(pair_tile.tolist(), pair_trace.tolist())) == \
+        set(zip(p_tile.tolist(), p_trace.tolist()))
+    assert int(seg_off[0]) == 0 and int(seg_off[-1]) == pair_trace.numel()
+    assert seg_off.numel() == seg_col.numel() + 1
+    assert torch.all(seg_col[1:] > seg_col[:-1])  # one segment per column, ascending
+    for g_ in range(seg_col.numel()):
+        a, b = int(seg_off[g_]), int(seg_off[g_ + 1])
+        assert b > a
+        assert torch.all(col[pair_trace[a:b].long()] == seg_col[g_])
