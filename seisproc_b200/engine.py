@@ -15,12 +15,16 @@ Reference behaviour kept:
   milestones of the reference.
 Coordinates given as float64 keep their precision: the grid origin is
 subtracted in float64 on the device before rounding to float32.
+
+``migrate_bin_time_domain_rms`` (:633-802) is the reference's time-domain RMS
+operator, a different operator, on its own kernel (``time_domain``); the other
+time-domain and own-midpoint entries raise ``NotImplementedError``.
 """
 from __future__ import annotations
 
 import logging
 import time
-from typing import Callable, Optional, Tuple, Union
+from typing import Callable, Optional, Tuple
 
 import numpy as np
 import torch
