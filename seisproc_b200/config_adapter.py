@@ -98,6 +98,33 @@ class ConfigAdapter:
             out["kernel_backend"] = self.config["kernel_backend"]
         return out
 
+    def get_time_domain_params(self, traces: np.ndarray, source_x: np.ndarray,
+                               source_y: np.ndarray, receiver_x: np.ndarray,
+                               receiver_y: np.ndarray, normalize: bool = True, min_fold: int = 1,
+                               progress_callback: Optional[Callable[[float, str], None]] = None,
+                               enable_profiling: bool = False,
+                               use_time_dependent_aperture: bool = True) -> Dict[str, Any]:
+        """The reference's kwargs for the time-domain entries
+        (config_adapter.py:239-304): the engine arguments with ``tile_size``
+        and a time-dependent aperture by default.  The batch worker takes the
+        grid keys from it for ``migrate_bin_time_domain_rms``
+        (views/migration_monitor_dialog.py:288-362), adding ``velocity_model``,
+        ``n_times`` and the params' ``tile_size``, ``sample_batch_size`` and
+        ``max_traces_per_tile``."""
+        p = self.params
+        return {
+            "traces": traces, "source_x": source_x, "source_y": source_y,
+            "receiver_x": receiver_x, "receiver_y": receiver_y,
+            "origin_x": p.origin_x, "origin_y": p.origin_y, "il_spacing": p.il_spacing,
+            "xl_spacing": p.xl_spacing, "azimuth_deg": p.azimuth_deg, "n_il": p.n_il,
+            "n_xl": p.n_xl, "dt_ms": p.dt_ms, "t_min_ms": p.t_min_ms, "n_times": p.n_samples,
+            "velocity_mps": p.velocity_mps, "max_aperture_m": p.max_aperture_m,
+            "max_angle_deg": p.max_angle_deg, "tile_size": p.tile_size,
+            "normalize": normalize, "min_fold": min_fold,
+            "progress_callback": progress_callback, "enable_profiling": enable_profiling,
+            "use_time_dependent_aperture": use_time_dependent_aperture,
+        }
+
     def validate(self) -> Tuple[bool, str]:
         issues = []
         c = self.config

@@ -160,3 +160,38 @@ def test_column_pairs_sorted_by_midpoint_column(name):
         a, b = int(seg_off[g_]), int(seg_off[g_ + 1])
         assert b > a
         assert torch.all(col[pair_trace[a:b].long()] == seg_col[g_])
+
+
+def test_config_adapter_time_domain_params():
+    """ConfigAdapter.get_time_domain_params gives the reference's keys and
+    values (its known answer, tests/test_time_domain_migration.py:362-402), and
+    the batch worker's migrate_bin_time_domain_rms call built from them
+    (views/migration_monitor_dialog.py:328-362) binds to the engine's signature."""
+    import inspect
+    from seisproc_b200.config_adapter import ConfigAdapter
+    from seisproc_b200.engine import MigrationEngine
+    from seisproc_b200.velocity import create_velocity_model
+    a = ConfigAdapter({"x_origin": 100.0, "y_origin": 200.0, "output_bin_il": 25.0,
+                       "output_bin_xl": 25.0, "inline_min": 1, "inline_max": 10,
+                       "xline_min": 1, "xline_max": 10, "dt_ms": 4.0, "time_min_ms": 0.0,
+                       "time_max_ms": 400.0, "velocity_v0": 2500.0, "max_aperture_m": 3000.0,
+                       "max_angle_deg": 60.0, "tile_size": 100})
+    z = np.zeros(50, np.float32)
+    tr = np.zeros((101, 50), np.float32)
+    params = a.get_time_domain_params(traces=tr, source_x=z, source_y=z, receiver_x=z,
+                                      receiver_y=z)
+    assert "n_times" in params and "tile_size" in params
+    assert params["n_times"] == 101
+    assert params["origin_x"] == 100.0 and params["origin_y"] == 200.0
+    assert params["use_time_dependent_aperture"] is True
+    p = a.params
+    worker_kwargs = dict(
+        traces=tr, source_x=z, source_y=z, receiver_x=z, receiver_y=z,
+        **{k: params[k] for k in ("origin_x", "origin_y", "il_spacing", "xl_spacing",
+                                  "azimuth_deg", "n_il", "n_xl", "dt_ms", "t_min_ms",
+                                  "max_aperture_m", "max_angle_deg")},
+        n_times=p.n_samples, velocity_model=create_velocity_model("gradient", 2500.0, 0.4),
+        tile_size=p.tile_size, sample_batch_size=p.sample_batch_size,
+        max_traces_per_tile=p.max_traces_per_tile, normalize=False,
+        progress_callback=None, enable_profiling=True, use_time_dependent_aperture=True)
+    inspect.signature(MigrationEngine.migrate_bin_time_domain_rms).bind(None, **worker_kwargs)
