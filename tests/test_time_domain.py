@@ -195,3 +195,20 @@ def test_config_adapter_time_domain_params():
         max_traces_per_tile=p.max_traces_per_tile, normalize=False,
         progress_callback=None, enable_profiling=True, use_time_dependent_aperture=True)
     inspect.signature(MigrationEngine.migrate_bin_time_domain_rms).bind(None, **worker_kwargs)
+
+
+def test_config_adapter_advanced_fields_and_defaults():
+    """The adapter's time-domain fields and their defaults, as the reference
+    pins them (tests/test_time_domain_migration.py:331-430)."""
+    from seisproc_b200.config_adapter import ConfigAdapter
+    base = {"x_origin": 0.0, "y_origin": 0.0, "output_bin_il": 25.0, "output_bin_xl": 25.0,
+            "inline_min": 1, "inline_max": 10, "xline_min": 1, "xline_max": 10, "dt_ms": 4.0,
+            "time_min_ms": 0.0, "time_max_ms": 400.0, "velocity_v0": 2500.0,
+            "max_aperture_m": 3000.0, "max_angle_deg": 60.0}
+    p = ConfigAdapter({**base, "tile_size": 200, "use_time_domain": True, "use_kdtree": True,
+                       "sample_batch_size": 150}).params
+    assert p.tile_size == 200 and p.use_time_domain is True and p.use_kdtree is True
+    assert p.sample_batch_size == 150
+    p = ConfigAdapter(base).params
+    assert p.tile_size == 100 and p.use_time_domain is False and p.use_kdtree is False
+    assert p.sample_batch_size == 200 and p.max_traces_per_tile == 5000
