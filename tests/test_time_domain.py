@@ -212,3 +212,25 @@ def test_config_adapter_advanced_fields_and_defaults():
     p = ConfigAdapter(base).params
     assert p.tile_size == 100 and p.use_time_domain is False and p.use_kdtree is False
     assert p.sample_batch_size == 200 and p.max_traces_per_tile == 5000
+
+
+def test_engine_velocity_model_known_answers():
+    """V_rms(t) of the engine's velocity model on scalars, arrays and float32
+    tensors, as the reference pins it (tests/test_velocity_model.py:95-150)."""
+    from seisproc_b200.velocity import VelocityModel
+    m = VelocityModel(velocity_type="gradient", v0=2000.0, gradient=0.5)
+    v = [m.rms_velocity_at_time(t) for t in (500.0, 1000.0, 2000.0)]
+    assert v[0] < v[1] < v[2]
+    assert m.rms_velocity_at_time(0.0) == 2000.0
+    t = torch.tensor([0.0, 500.0, 1000.0, 2000.0], dtype=torch.float32)
+    vt = m.rms_velocity_at_time(t)
+    assert isinstance(vt, torch.Tensor) and vt.shape == (4,) and vt.dtype == torch.float32
+    assert torch.isclose(vt[0], torch.tensor(2000.0))
+    assert (vt[1:] > vt[:-1]).all()
+    # the float32 tensor branch and the float64 array branch agree to rounding
+    np.testing.assert_allclose(vt.numpy(), m.rms_velocity_at_time(t.numpy()), rtol=1e-6)
+    z = VelocityModel(velocity_type="gradient", v0=2500.0, gradient=0.0)
+    assert np.allclose(z.rms_velocity_at_time(np.array([0, 500, 1000, 2000])), 2500.0)
+    assert torch.all(z.rms_velocity_at_time(t) == 2500.0)
+    s = VelocityModel(velocity_type="gradient", v0=1500.0, gradient=0.5)
+    assert 1500.0 < s.rms_velocity_at_time(2000.0) < 2500.0
