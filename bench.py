@@ -691,6 +691,91 @@ def bench_velocity(args):
     }), flush=True)
 
 
+TR_SPACING, TR_DT, TR_APERTURE, TR_ANGLE = 25.0, 4.0, 1000.0, 60.0
+TR_V0, TR_GRADIENT = 1500.0, 0.6
+
+
+def time_rms_survey(n_tr: int, n_s: int):
+    """The time_rms workload's seeded traces and coordinates (float32 numpy):
+    midpoints uniform over 5 x 5 km, offsets uniform 0-3 km, azimuths uniform,
+    Gaussian traces (n_s, n_tr)."""
+    rs = np.random.RandomState(2025)
+    mx, my = rs.uniform(0, 5000, n_tr), rs.uniform(0, 5000, n_tr)
+    off, phi = rs.uniform(0, 3000, n_tr), rs.uniform(0, 2 * np.pi, n_tr)
+    sx = (mx - 0.5 * off * np.cos(phi)).astype(np.float32)
+    sy = (my - 0.5 * off * np.sin(phi)).astype(np.float32)
+    rx = (mx + 0.5 * off * np.cos(phi)).astype(np.float32)
+    ry = (my + 0.5 * off * np.sin(phi)).astype(np.float32)
+    tr = rs.standard_normal((n_s, n_tr)).astype(np.float32)
+    return tr, sx, sy, rx, ry
+
+
+def time_rms_workload(n_tr: int, n_s: int, n: int) -> str:
+    return (f"time-domain RMS operator, {n_tr} traces x {n_s} samples, {n}x{n}x{n_s} output "
+            f"grid, aperture {TR_APERTURE:.0f} m, {TR_ANGLE:.0f} deg, tiles of 100 points, "
+            "5000-trace cap")
+
+
+def time_rms_cpu_sample(tr, sx, sy, rx, ry, n: int, n_s: int, max_traces: int = 500):
+    """The float32 oracle on a bounded sample of the time_rms workload: the
+    first tile (100 output points) with the first ``max_traces`` (by index) of
+    the traces the reference lists for it.  Returns (evaluated triples,
+    seconds, description); triples count the (point, trace) pairs inside the
+    aperture times the input samples, as the kernel's metric does."""
+    import torch as _t
+    from oracle import time_domain as otd
+    from seisproc_b200.velocity import VelocityModel
+    f32 = np.float32
+    ox, oy = otd.output_grid_f32(12.5, 12.5, TR_SPACING, TR_SPACING, 0.0, n, n)
+    tile = otd.effective_tile_size(100, 5000, 200)
+    mx, my = (sx + rx) / f32(2), (sy + ry) / f32(2)
+    (_, _, sel), = otd.tile_trace_lists(ox[:tile], oy[:tile], mx, my, tile, TR_APERTURE, 5000)
+    sel = np.sort(sel)[:max_traces]
+    if sel.size == 0:
+        raise RuntimeError("the first tile lists no traces")
+    pts = np.arange(min(tile, n * n))
+    hh = np.sqrt((ox[pts, None] - mx[None, sel]) ** 2 + (oy[pts, None] - my[None, sel]) ** 2)
+    evals = int((hh < TR_APERTURE).sum()) * n_s
+    t_in = _t.arange(n_s, dtype=_t.float32) * TR_DT
+    v_in = VelocityModel("gradient", TR_V0, gradient=TR_GRADIENT).rms_velocity_at_time(t_in)
+    t0 = time.perf_counter()
+    otd.time_domain_rms_f32(tr, sx, sy, rx, ry, v_in.numpy(), 12.5, 12.5, TR_SPACING,
+                            TR_SPACING, 0.0, n, n, TR_DT, 0.0, n_s, TR_APERTURE, TR_ANGLE,
+                            tiles=[(int(pts[0]), int(pts[-1]) + 1, sel)])
+    sec = time.perf_counter() - t0
+    return evals, sec, (f"first tile: {pts.size} points x {sel.size} of its traces x {n_s} "
+                        "samples, float32 numpy oracle")
+
+
+def bench_time_rms_reference(args):
+    """Reference arm of the time_rms config: the float32 oracle (the
+    reference's time-domain RMS algorithm restated, kind "port"; the reference
+    itself does not travel) on the bounded sample of ``time_rms_cpu_sample``,
+    one sample per step, on rank 0 only."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    n_tr, n_s, n = args.traces, args.samples, args.grid
+    tr, sx, sy, rx, ry = time_rms_survey(n_tr, n_s)
+    vals, secs = [], []
+    for i in range(args.warmup + args.steps):
+        ev, sec, sample = time_rms_cpu_sample(tr, sx, sy, rx, ry, n, n_s)
+        if i >= args.warmup:
+            vals.append(ev / sec / 1e9)
+            secs.append(sec)
+    v = statistics.median(vals)
+    print(json.dumps({
+        "metric": "time-domain RMS scatter Gevals/s", "value": v, "unit": "Gevals/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": statistics.median(secs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference", "config": {"workload": time_rms_workload(n_tr, n_s, n)},
+        "cpu_baseline": {"value": v, "unit": "Gevals/s", "cores": 1, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "Gevals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
 def bench_time_rms(args):
     """The time-domain RMS operator (MigrationEngine.migrate_bin_time_domain_rms)
     on the 3D survey's geometry: N traces with midpoints over 5 x 5 km, offsets
@@ -707,22 +792,13 @@ def bench_time_rms(args):
     from seisproc_b200 import time_domain as TD
     from seisproc_b200.engine import MigrationEngine
     from seisproc_b200.velocity import VelocityModel
-    sys.path.insert(0, ROOT)
-    from oracle import time_domain as otd
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
     L = _lib.lib()
     n_tr, n_s, n = args.traces, args.samples, args.grid
-    sp, dt, A, theta = 25.0, 4.0, 1000.0, 60.0
-    rs = np.random.RandomState(2025)
-    mx, my = rs.uniform(0, 5000, n_tr), rs.uniform(0, 5000, n_tr)
-    off, phi = rs.uniform(0, 3000, n_tr), rs.uniform(0, 2 * np.pi, n_tr)
-    sx = (mx - 0.5 * off * np.cos(phi)).astype(np.float32)
-    sy = (my - 0.5 * off * np.sin(phi)).astype(np.float32)
-    rx = (mx + 0.5 * off * np.cos(phi)).astype(np.float32)
-    ry = (my + 0.5 * off * np.sin(phi)).astype(np.float32)
-    tr = rs.standard_normal((n_s, n_tr)).astype(np.float32)
-    vm = VelocityModel("gradient", 1500.0, gradient=0.6)
+    sp, dt, A, theta = TR_SPACING, TR_DT, TR_APERTURE, TR_ANGLE
+    tr, sx, sy, rx, ry = time_rms_survey(n_tr, n_s)
+    vm = VelocityModel("gradient", TR_V0, gradient=TR_GRADIENT)
     grid = dict(origin_x=12.5, origin_y=12.5, il_spacing=sp, xl_spacing=sp, azimuth_deg=0.0,
                 n_il=n, n_xl=n, dt_ms=dt, t_min_ms=0.0, n_times=n_s)
     # resident inputs, built once as the engine builds them
@@ -798,25 +874,12 @@ def bench_time_rms(args):
             normalize=False, **grid)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e = statistics.median(e2e_ms)
-    # CPU: the float32 oracle on the first tile with pairs (500 of its traces),
-    # scaled per evaluation
+    # CPU: the float32 oracle on a sample of the same workload
     cpu = None
     if not args.no_cpu:
-        t_sel = int(p_tile[0])
-        sel = p_trace[p_tile == t_sel].cpu().numpy()[:500]
-        pts = np.arange(t_sel * tile, min((t_sel + 1) * tile, n * n))
-        oxn, oyn = ox.cpu().numpy(), oy.cpu().numpy()
-        mxn, myn = mid_x.cpu().numpy(), mid_y.cpu().numpy()
-        hh = np.sqrt((oxn[pts, None] - mxn[None, sel]) ** 2 + (oyn[pts, None] - myn[None, sel]) ** 2)
-        ev_cpu = int((hh < A).sum()) * n_s
-        v_in = vm.rms_velocity_at_time(t_axis.cpu()).numpy()
-        t0 = time.perf_counter()
-        otd.time_domain_rms_f32(tr, sx, sy, rx, ry, v_in, 12.5, 12.5, sp, sp, 0.0, n, n, dt,
-                                0.0, n_s, A, theta, tiles=[(pts[0], pts[-1] + 1, sel)])
-        cpu_s = time.perf_counter() - t0
+        ev_cpu, cpu_s, sample = time_rms_cpu_sample(tr, sx, sy, rx, ry, n, n_s)
         cpu = {"value": ev_cpu / cpu_s / 1e9, "unit": "Gevals/s", "cores": 1, "kind": "port",
-               "sample": f"one tile: {pts.size} points x {sel.size} of its traces x {n_s} samples, "
-                         "float32 numpy oracle"}
+               "sample": sample}
     pk = peaks()
     mufu_peak = 148 * 16 * pk["sm_max_mhz"] * 1e6 / 8 / 1e9  # Gevals/s
     val = evals / (kern_ms * 1e-3) / 1e9
@@ -825,9 +888,7 @@ def bench_time_rms(args):
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": kern_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"time-domain RMS operator, {n_tr} traces x {n_s} samples, "
-                               f"{n}x{n}x{n_s} output grid, aperture {A:.0f} m, {theta:.0f} deg, "
-                               "tiles of 100 points, 5000-trace cap",
+        "config": {"workload": time_rms_workload(n_tr, n_s, n),
                    "pairs": int(p_tile.numel()), "evals": evals,
                    "l2": "inputs (traces 2 GB) larger than L2"},
         "call_ms": call_ms, "call_fold_matches_kernel_run": same,
@@ -874,8 +935,8 @@ def main():
         return bench_lsq(args)
     if args.config == "velocity" and args.impl == "ours":
         return bench_velocity(args)
-    if args.config == "time_rms" and args.impl == "ours":
-        return bench_time_rms(args)
+    if args.config == "time_rms":
+        return bench_time_rms(args) if args.impl == "ours" else bench_time_rms_reference(args)
     if args.impl == "reference":
         bench_reference(args)
     else:

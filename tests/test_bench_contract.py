@@ -46,3 +46,16 @@ def test_reference_arm_unavailable_for_antialias():
     lines = _run(["--impl", "reference", "--antialias"])
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and "unavailable" in d
+
+
+def test_time_rms_reference_arm_json_line():
+    """--config time_rms --impl reference times the float32 oracle on the same
+    workload with the same metric as the GPU arm."""
+    lines = _run(["--config", "time_rms", "--impl", "reference", "--steps", "1", "--warmup",
+                  "0", "--traces", "8000", "--samples", "100", "--grid", "20"])
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == "time-domain RMS scatter Gevals/s"
+    assert d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
+    assert d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["config"]["workload"].startswith("time-domain RMS operator, 8000 traces")
