@@ -605,6 +605,67 @@ def bench_lsq(args):
     plan.close()
 
 
+def velocity_case(n_t: int, n: int):
+    """The velocity config's picked cube (43 x 23 x 23 nodes: every 100 ms and
+    250 m, seeded) and the output grid's times and column coordinates."""
+    rs = np.random.RandomState(5)
+    z = np.linspace(0.0, 4.2, 43).astype(np.float32)          # picks every 100 ms
+    x = np.linspace(-250.0, 5250.0, 23).astype(np.float32)    # nodes every 250 m
+    y = np.linspace(-250.0, 5250.0, 23).astype(np.float32)
+    cube = (1500 + 500 * z[:, None, None] + 0.02 * x[None, :, None] + 0.01 * y[None, None, :]
+            + rs.uniform(-25, 25, (z.size, x.size, y.size))).astype(np.float32)
+    t_s = np.arange(n_t) * 0.004
+    il = np.arange(n)[:, None]
+    xl = np.arange(n)[None, :]
+    cx = (12.5 + 25.0 * il + 0 * xl).ravel()
+    cy = (12.5 + 0 * il + 25.0 * xl).ravel()
+    return z, x, y, cube, t_s, cx, cy
+
+
+def bench_velocity_reference(args):
+    """Reference arm of the velocity config: the reference's evaluation
+    (models/velocity_model.py:181-245, scipy RegularGridInterpolator, linear,
+    extrapolating) at every output time of every 50th column, on rank 0."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from scipy.interpolate import RegularGridInterpolator
+    n_t, n = args.samples, args.grid
+    z, x, y, cube, t_s, cx, cy = velocity_case(n_t, n)
+    sel = np.arange(0, n * n, 50)
+    f = RegularGridInterpolator((z, x, y), cube, method="linear", bounds_error=False,
+                                fill_value=None)
+    pts = np.stack(np.broadcast_arrays(t_s[:, None], cx[sel][None, :], cy[sel][None, :]),
+                   -1).reshape(-1, 3)
+    vals, secs = [], []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        f(pts).astype(np.float32)
+        sec = time.perf_counter() - t0
+        if i >= args.warmup:
+            vals.append(pts.shape[0] / sec / 1e9)
+            secs.append(sec)
+    v = statistics.median(vals)
+    print(json.dumps({
+        "metric": "V_rms grid Gsamples/s", "value": v, "unit": "Gsamples/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": statistics.median(secs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 blend, f32 out",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"3-D velocity cube {z.size}x{x.size}x{y.size} nodes resampled "
+                               f"onto the {n}x{n}x{n_t} output grid"},
+        "cpu_baseline": {"value": v, "unit": "Gsamples/s", "cores": 1, "kind": "port",
+                         "sample": f"{sel.size} of {n * n} columns x {n_t} times, scipy "
+                                   "RegularGridInterpolator"},
+        "e2e": {"value": v, "unit": "Gsamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def bench_unavailable(why: str):
+    if int(os.environ.get("RANK", "0")) == 0:
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+
+
 def bench_velocity(args):
     """V_rms ingestion: a picked 3-D velocity cube (coarse nodes, as an
     IL-XL-T-V or SEG-Y velocity file gives) resampled onto every sample of the
@@ -620,18 +681,8 @@ def bench_velocity(args):
     dev = torch.device("cuda", 0)
     L = _lib.lib()
     n_t, n = args.samples, args.grid
-    rs = np.random.RandomState(5)
-    z = np.linspace(0.0, 4.2, 43).astype(np.float32)          # picks every 100 ms
-    x = np.linspace(-250.0, 5250.0, 23).astype(np.float32)    # nodes every 250 m
-    y = np.linspace(-250.0, 5250.0, 23).astype(np.float32)
-    cube = (1500 + 500 * z[:, None, None] + 0.02 * x[None, :, None] + 0.01 * y[None, None, :]
-            + rs.uniform(-25, 25, (z.size, x.size, y.size))).astype(np.float32)
+    z, x, y, cube, t_s, cx, cy = velocity_case(n_t, n)
     m = M.create_3d_velocity(cube, z, x, y)
-    t_s = np.arange(n_t) * 0.004
-    il = np.arange(n)[:, None]
-    xl = np.arange(n)[None, :]
-    cx = (12.5 + 25.0 * il + 0 * xl).ravel()
-    cy = (12.5 + 0 * il + 25.0 * xl).ravel()
     g = VelocityGridder(m, t_s, cx, cy, dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > L2
     for _ in range(args.warmup):
@@ -929,12 +980,19 @@ def main():
     ap.add_argument("--config", default="3d",
                     choices=["3d", "batched", "lsq", "velocity", "time_rms"])
     args = ap.parse_args()
-    if args.config == "batched" and args.impl == "ours":
-        return bench_batched(args)
-    if args.config == "lsq" and args.impl == "ours":
-        return bench_lsq(args)
-    if args.config == "velocity" and args.impl == "ours":
-        return bench_velocity(args)
+    if args.config == "batched":
+        if args.impl == "ours":
+            return bench_batched(args)
+        return bench_unavailable("the reference migrates offset/azimuth classes one bin at a "
+                                 "time through migrate_bin_full; its per-bin arm is the default "
+                                 "config")
+    if args.config == "lsq":
+        if args.impl == "ours":
+            return bench_lsq(args)
+        return bench_unavailable("the reference has no demigration (adjoint) and no "
+                                 "least-squares migration")
+    if args.config == "velocity":
+        return bench_velocity(args) if args.impl == "ours" else bench_velocity_reference(args)
     if args.config == "time_rms":
         return bench_time_rms(args) if args.impl == "ours" else bench_time_rms_reference(args)
     if args.impl == "reference":

@@ -59,3 +59,15 @@ def test_time_rms_reference_arm_json_line():
     assert d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["config"]["workload"].startswith("time-domain RMS operator, 8000 traces")
+
+
+def test_velocity_reference_arm_and_unavailable_configs():
+    lines = _run(["--config", "velocity", "--impl", "reference", "--steps", "1", "--warmup",
+                  "0", "--samples", "100", "--grid", "20"])
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == "V_rms grid Gsamples/s"
+    assert d["value"] > 0 and "RegularGridInterpolator" in d["cpu_baseline"]["sample"]
+    for cfg in ("lsq", "batched"):
+        d = json.loads(_run(["--config", cfg, "--impl", "reference"])[0])
+        assert d["impl"] == "reference" and d["unavailable"]
+    assert _run(["--config", "lsq", "--impl", "reference"], env={"RANK": "1"}) == []
