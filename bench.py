@@ -767,21 +767,23 @@ def time_rms_workload(n_tr: int, n_s: int, n: int) -> str:
             "5000-trace cap")
 
 
-def time_rms_cpu_sample(tr, sx, sy, rx, ry, n: int, n_s: int, max_traces: int = 500):
-    """The float32 oracle on a bounded sample of the time_rms workload: the
-    first tile (100 output points) with the first ``max_traces`` (by index) of
-    the traces the reference lists for it.  Returns (evaluated triples,
-    seconds, description); triples count the (point, trace) pairs inside the
-    aperture times the input samples, as the kernel's metric does."""
+def time_rms_cpu_sample(tr, sx, sy, rx, ry, n: int, n_s: int):
+    """The reference's time-domain computation on the host cores (the oracle's
+    bit-identical torch port, all threads) on a bounded sample of the time_rms
+    workload: its first tile (100 output points) with every trace the
+    reference lists for it.  Returns (evaluated triples, seconds, description,
+    threads); triples count the (point, trace) pairs inside the aperture times
+    the input samples, as the kernel's metric does."""
     import torch as _t
     from oracle import time_domain as otd
     from seisproc_b200.velocity import VelocityModel
+    threads = len(os.sched_getaffinity(0))
+    _t.set_num_threads(threads)
     f32 = np.float32
     ox, oy = otd.output_grid_f32(12.5, 12.5, TR_SPACING, TR_SPACING, 0.0, n, n)
     tile = otd.effective_tile_size(100, 5000, 200)
     mx, my = (sx + rx) / f32(2), (sy + ry) / f32(2)
     (_, _, sel), = otd.tile_trace_lists(ox[:tile], oy[:tile], mx, my, tile, TR_APERTURE, 5000)
-    sel = np.sort(sel)[:max_traces]
     if sel.size == 0:
         raise RuntimeError("the first tile lists no traces")
     pts = np.arange(min(tile, n * n))
@@ -790,26 +792,27 @@ def time_rms_cpu_sample(tr, sx, sy, rx, ry, n: int, n_s: int, max_traces: int = 
     t_in = _t.arange(n_s, dtype=_t.float32) * TR_DT
     v_in = VelocityModel("gradient", TR_V0, gradient=TR_GRADIENT).rms_velocity_at_time(t_in)
     t0 = time.perf_counter()
-    otd.time_domain_rms_f32(tr, sx, sy, rx, ry, v_in.numpy(), 12.5, 12.5, TR_SPACING,
-                            TR_SPACING, 0.0, n, n, TR_DT, 0.0, n_s, TR_APERTURE, TR_ANGLE,
-                            tiles=[(int(pts[0]), int(pts[-1]) + 1, sel)])
+    otd.time_domain_rms_torch_port(tr, sx, sy, rx, ry, ox, oy, n_s, v_in.numpy(), TR_DT, 0.0,
+                                   TR_APERTURE, TR_ANGLE, n, n, 12.5, 12.5, TR_SPACING,
+                                   TR_SPACING, 0.0, first_tile=0, n_tiles=1)
     sec = time.perf_counter() - t0
-    return evals, sec, (f"first tile: {pts.size} points x {sel.size} of its traces x {n_s} "
-                        "samples, float32 numpy oracle")
+    return evals, sec, (f"first tile: {pts.size} points x its {sel.size} listed traces x "
+                        f"{n_s} samples, the reference's float32 torch loop (oracle port), "
+                        f"{threads} threads"), threads
 
 
 def bench_time_rms_reference(args):
-    """Reference arm of the time_rms config: the float32 oracle (the
-    reference's time-domain RMS algorithm restated, kind "port"; the reference
-    itself does not travel) on the bounded sample of ``time_rms_cpu_sample``,
-    one sample per step, on rank 0 only."""
+    """Reference arm of the time_rms config: the reference's float32 torch
+    loop (the oracle's bit-identical port, kind "port"; the reference itself
+    does not travel) on the bounded sample of ``time_rms_cpu_sample``, one
+    sample per step, all host threads, on rank 0 only."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     n_tr, n_s, n = args.traces, args.samples, args.grid
     tr, sx, sy, rx, ry = time_rms_survey(n_tr, n_s)
     vals, secs = [], []
     for i in range(args.warmup + args.steps):
-        ev, sec, sample = time_rms_cpu_sample(tr, sx, sy, rx, ry, n, n_s)
+        ev, sec, sample, threads = time_rms_cpu_sample(tr, sx, sy, rx, ry, n, n_s)
         if i >= args.warmup:
             vals.append(ev / sec / 1e9)
             secs.append(sec)
@@ -820,7 +823,7 @@ def bench_time_rms_reference(args):
         "ms_per_step": statistics.median(secs) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "reference", "config": {"workload": time_rms_workload(n_tr, n_s, n)},
-        "cpu_baseline": {"value": v, "unit": "Gevals/s", "cores": 1, "kind": "port",
+        "cpu_baseline": {"value": v, "unit": "Gevals/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": v, "unit": "Gevals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -928,9 +931,9 @@ def bench_time_rms(args):
     # CPU: the float32 oracle on a sample of the same workload
     cpu = None
     if not args.no_cpu:
-        ev_cpu, cpu_s, sample = time_rms_cpu_sample(tr, sx, sy, rx, ry, n, n_s)
-        cpu = {"value": ev_cpu / cpu_s / 1e9, "unit": "Gevals/s", "cores": 1, "kind": "port",
-               "sample": sample}
+        ev_cpu, cpu_s, sample, threads = time_rms_cpu_sample(tr, sx, sy, rx, ry, n, n_s)
+        cpu = {"value": ev_cpu / cpu_s / 1e9, "unit": "Gevals/s", "cores": threads,
+               "kind": "port", "sample": sample}
     pk = peaks()
     mufu_peak = 148 * 16 * pk["sm_max_mhz"] * 1e6 / 8 / 1e9  # Gevals/s
     val = evals / (kern_ms * 1e-3) / 1e9

@@ -169,3 +169,92 @@ def rms_velocity_torch_order_f32(velocity_type, v0, gradient, t_ms):
     vs = f32(v0 * v0) + f32(v0 * k) * z + (f32(k * k) * z * z) / f32(3.0)
     v = np.sqrt(np.maximum(vs, f32(v0 * v0 * 0.5)))
     return np.where(t < f32(1.0), f32(v0), v).astype(f32)
+
+
+def time_domain_rms_torch_port(traces, source_x, source_y, receiver_x, receiver_y, output_x,
+                               output_y, n_times, v_rms_in, dt_ms, t_min_ms, max_aperture_m,
+                               max_angle_deg, n_il, n_xl, origin_x, origin_y, il_spacing,
+                               xl_spacing, azimuth_deg, tile_size=100, sample_batch_size=200,
+                               max_traces_per_tile=5000, use_time_dependent_aperture=True,
+                               first_tile=0, n_tiles=None):
+    """The reference's own float32 torch computation, run on the CPU in the
+    reference's order, for a bit-identical result and a faithful CPU timing.
+
+    Steps as kirchhoff_kernel.py:1410-1700 takes them: per tile of consecutive
+    output points the midpoint pre-filter and the nearest-``max_traces_per_tile``
+    cap (same ``torch.argsort`` call, so ties fall the same way), the input
+    samples in batches sized by the reference's memory rule (:1604-1616), the
+    per-sample terms of :1243-1282 as whole-tensor float32 operations, and one
+    ``scatter_add_`` per batch into the flattened image and fold (the order of
+    the float32 sums).  ``first_tile`` / ``n_tiles`` restrict it to a run of
+    tiles (a bounded CPU sample).  Returns float32 torch tensors
+    (n_times, n_il, n_xl)."""
+    import torch
+    f = torch.float32
+    tr = torch.as_tensor(np.asarray(traces, np.float32))
+    sx, sy, rx, ry = (torch.as_tensor(np.asarray(a, np.float32))
+                      for a in (source_x, source_y, receiver_x, receiver_y))
+    ox = torch.as_tensor(np.asarray(output_x, np.float32))
+    oy = torch.as_tensor(np.asarray(output_y, np.float32))
+    v = torch.as_tensor(np.asarray(v_rms_in, np.float32))
+    n_s = tr.shape[0]
+    n_out = n_il * n_xl
+    mid_x, mid_y = (sx + rx) / 2.0, (sy + ry) / 2.0
+    hoff_sq = ((rx - sx) / 2.0) ** 2 + ((ry - sy) / 2.0) ** 2
+    cos_az, sin_az = np.cos(np.radians(azimuth_deg)), np.sin(np.radians(azimuth_deg))
+    ddx, ddy = mid_x - origin_x, mid_y - origin_y
+    t_il = ((ddx * cos_az + ddy * sin_az) / il_spacing).long().clamp(0, n_il - 1)
+    t_xl = ((-ddx * sin_az + ddy * cos_az) / xl_spacing).long().clamp(0, n_xl - 1)
+    theta = np.radians(max_angle_deg)
+    tan_t = np.tan(theta)
+    tile = effective_tile_size(tile_size, max_traces_per_tile, sample_batch_size)
+    max_el = int(12.0 * 1024 ** 3 / 4 / 10)
+    image = torch.zeros(n_times * n_out, dtype=f)
+    fold = torch.zeros(n_times * n_out, dtype=f)
+    starts = list(range(0, n_out, tile))[first_tile:]
+    if n_tiles is not None:
+        starts = starts[:n_tiles]
+    with torch.no_grad():
+        for a in starts:
+            b = min(a + tile, n_out)
+            tx, ty = ox[a:b], oy[a:b]
+            cx = (tx.min() + tx.max()) / 2
+            cy = (ty.min() + ty.max()) / 2
+            rad = torch.sqrt(((tx - cx) ** 2 + (ty - cy) ** 2).max())
+            dist = torch.sqrt((mid_x - cx) ** 2 + (mid_y - cy) ** 2)
+            sel = torch.where(dist < (max_aperture_m + rad + 100))[0]
+            if sel.numel() == 0:
+                continue
+            if sel.numel() > max_traces_per_tile:
+                sel = sel[torch.argsort(dist[sel])[:max_traces_per_tile]]
+            n_f, n_p = sel.numel(), b - a
+            h_sq = (tx[:, None] - mid_x[sel][None, :]) ** 2 + (ty[:, None] - mid_y[sel][None, :]) ** 2
+            h = torch.sqrt(h_sq)[None]
+            c = (h_sq + hoff_sq[sel][None, :])[None]
+            h_sq = h_sq[None]
+            cols = (t_il[sel] * n_xl + t_xl[sel]).view(1, 1, n_f)
+            sb = min(sample_batch_size, max(10, max_el // max(1, n_p * n_f)), n_s)
+            for s0 in range(0, n_s, sb):
+                s1 = min(s0 + sb, n_s)
+                t_in = 0.0 + torch.arange(s0, s1, dtype=f) * dt_ms
+                vb = v[s0:s1]
+                v_out = vb.view(-1, 1, 1).expand(s1 - s0, n_p, n_f)
+                t_out = torch.sqrt((t_in ** 2).view(-1, 1, 1)
+                                   + 4.0 * c * 1e6 / (vb ** 2).view(-1, 1, 1))
+                o_idx = (t_out - t_min_ms) / dt_ms
+                keep = (o_idx >= 0) & (o_idx < n_times - 0.001)
+                if use_time_dependent_aperture:
+                    keep = keep & (h < torch.clamp(t_out * v_out / 2000.0 * tan_t,
+                                                   max=max_aperture_m))
+                else:
+                    keep = keep & (h < max_aperture_m)
+                z = v_out * t_out / 2000.0
+                keep = keep & (torch.atan2(h, z + 1e-6) < theta)
+                r2 = z ** 2 + h_sq
+                w = z / (torch.sqrt(r2) * r2 + 1e-10)
+                amp = tr[s0:s1][:, sel].unsqueeze(1).expand(-1, n_p, -1)
+                contrib = amp * w * keep.float()
+                lin = o_idx.long().clamp(0, n_times - 1) * n_out + cols
+                image.scatter_add_(0, lin.reshape(-1), contrib.reshape(-1))
+                fold.scatter_add_(0, lin.reshape(-1), keep.reshape(-1).float())
+    return image.view(n_times, n_il, n_xl), fold.view(n_times, n_il, n_xl)
