@@ -282,8 +282,10 @@ typedef struct pstm_time_rms_params {
  * masked by output range, aperture and angle, weighted by z / (r^3 + 1e-10),
  * and added at the truncated output index into the TRACE's own midpoint
  * column, with fold counted alongside.  The index arithmetic is the
- * reference's float32 sequence, so every contribution lands where the
- * reference puts it.
+ * reference's float32 sequence with IEEE rounding, so a contribution lands
+ * where the reference puts it except in the rare cases where the reference's
+ * CPU square root (torch's, not correctly rounded on every input) rounds an
+ * output time across an integer index.
  *
  * Device pointers: traces (n_samples, n_traces) float32 sample-major;
  * mid_x/mid_y/half_offset_sq per trace; out_x/out_y per output point; v_rms

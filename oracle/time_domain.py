@@ -16,10 +16,15 @@ reference's float32 operations in the reference's order (every Python scalar
 is rounded to float32 first, as torch does), which makes the output indices
 bit-identical, and accumulates the sums in float64.
 
-The angle mask uses ``np.arctan2`` in float32 where the reference uses torch's;
-both are within an ulp or two, so a pair exactly at the angle limit may fall
-on either side.  Pinned by golden vectors made by running the reference
-(tests/golden/make_time_domain_golden.py).
+Square roots here are IEEE (numpy's, as on a GPU); the reference's CPU run
+takes torch's CPU float32 sqrt, which is an ulp off on about 0.7 % of inputs,
+so where such an ulp straddles an integer output index the reference puts
+the contribution one sample over (a few dozen of 4e7 fold counts on a
+3000-trace case).  ``time_domain_rms_torch_port`` below repeats the reference
+with torch itself and is bit-identical to it.  The angle mask uses
+``np.arctan2`` where the reference uses torch's; they differ by an ulp on many
+inputs but moved no contribution in the cases measured.  Pinned by golden
+vectors made by running the reference (tests/golden/make_time_domain_golden.py).
 """
 from __future__ import annotations
 
@@ -156,9 +161,13 @@ def time_domain_rms_f32(traces, source_x, source_y, receiver_x, receiver_y, v_rm
 
 
 def rms_velocity_torch_order_f32(velocity_type, v0, gradient, t_ms):
-    """V_rms(t) the way the reference evaluates it on a float32 torch tensor
-    (processors/migration/velocity_model.py:109-175): constant v0; for a
-    gradient, float32 operations in the reference's order."""
+    """V_rms(t) the way the reference evaluates it on a float32 CPU torch
+    tensor (processors/migration/velocity_model.py:109-175): constant v0; for
+    a gradient, float32 operations in the reference's order.  The final square
+    root is torch's CPU float32 sqrt, which is not correctly rounded on every
+    input (an ulp off on about 0.7 % of them), so np.sqrt would not reproduce
+    the reference's table bit for bit."""
+    import torch
     t = np.asarray(t_ms, f32)
     if velocity_type == "constant" or abs(gradient) < 1e-10:
         return np.full(t.shape, v0, f32)
@@ -167,7 +176,7 @@ def rms_velocity_torch_order_f32(velocity_type, v0, gradient, t_ms):
     z = f32(v0) * tw + f32(0.5 * k * v0) * tw * tw
     z = np.maximum(z, f32(0))
     vs = f32(v0 * v0) + f32(v0 * k) * z + (f32(k * k) * z * z) / f32(3.0)
-    v = np.sqrt(np.maximum(vs, f32(v0 * v0 * 0.5)))
+    v = torch.sqrt(torch.from_numpy(np.maximum(vs, f32(v0 * v0 * 0.5)))).numpy()
     return np.where(t < f32(1.0), f32(v0), v).astype(f32)
 
 

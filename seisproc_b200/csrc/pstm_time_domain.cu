@@ -8,9 +8,11 @@
 // _time_domain_batch_kernel :1217-1287), a different operator from the
 // Kirchhoff summation of pstm_gather2.cuh.  Its output time index truncates a
 // float32 expression, so the index arithmetic here repeats the reference's
-// float32 operations in the reference's order with explicitly rounded
-// intrinsics (no FMA contraction): the index of every contribution is the
-// reference's, bit for bit.  The sums differ only in order.
+// float32 operations in the reference's order with explicitly rounded IEEE
+// intrinsics (no FMA contraction): each contribution lands at the reference's
+// index, except where torch's CPU float32 sqrt (not correctly rounded on
+// every input) rounds t_out across an integer index in the reference's own
+// CPU run -- a few in 10^7.  The sums differ only in order.
 //
 // Work split.  All contributions of a trace land in ONE column (its midpoint
 // bin), so the caller's (tile, trace) pairs are sorted by that column and a CTA

@@ -2,7 +2,7 @@
 
     PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_time_domain_golden.py /path/to/reference
 
-Writes ``time_domain_rms.npz``: three seeded surveys migrated by the reference's
+Writes ``time_domain_rms.npz``: four seeded surveys migrated by the reference's
 ``MigrationEngine.migrate_bin_time_domain_rms``
 (processors/migration/migration_engine.py:633-802, kernel
 kirchhoff_kernel.py:1313-1783) on the CPU:
@@ -11,7 +11,9 @@ kirchhoff_kernel.py:1313-1783) on the CPU:
 * ``c1``: linear-gradient V, rotated grid (30 deg), t_min 40 ms, fixed
   aperture, a trace cap of 40 per tile (the cap is active), small tiles;
 * ``c2``: tabulated v(z), more output times than input samples, normalised
-  by fold with min_fold 2.
+  by fold with min_fold 2;
+* ``c3``: dt 3 ms (the index division is not a power of two), fractional
+  t_min, 45 deg grid, a decreasing gradient V, an 85 deg angle limit, cap 60.
 
 For each case it stores the inputs (the parameters as ``cases_json``), the
 reference's V_rms at the input times, and the image and fold.  The reference
@@ -46,6 +48,10 @@ CASES = {
                origin=(0.0, 0.0), azimuth_deg=0.0, dt_ms=2.0, t_min_ms=0.0, n_times=110,
                vel=("file", 1600.0, 0.0), max_aperture_m=500.0, max_angle_deg=65.0,
                tile_size=100, max_traces_per_tile=5000, tda=True, normalize=True, min_fold=2),
+    "c3": dict(seed=14, n_tr=160, n_s=90, n_il=7, n_xl=11, il_spacing=22.5, xl_spacing=17.5,
+               origin=(-340.25, 812.5), azimuth_deg=45.0, dt_ms=3.0, t_min_ms=6.5, n_times=95,
+               vel=("gradient", 2100.0, -0.3), max_aperture_m=700.0, max_angle_deg=85.0,
+               tile_size=30, max_traces_per_tile=60, tda=True, normalize=False, min_fold=1),
 }
 
 FILE_Z = np.array([0.0, 150.0, 400.0, 900.0, 2000.0], np.float32)

@@ -1,10 +1,11 @@
 """Time-domain RMS operator on the GPU (pstm_time_rms_migrate) against the
 reference's own results (golden vectors) and the float32 oracle.
 
-The output index of every contribution is the reference's float32 expression,
-so folds agree exactly; the only allowed difference is a pair whose angle is
-within an ulp or two of the limit (atan2f here, torch's atan2 in the
-reference), which moves one count -- at most two such entries per case.  The
+The output index of every contribution is the reference's float32 expression
+with IEEE rounding, so folds agree except where a rounding the reference takes
+differently moves one count: torch's CPU float32 sqrt (not correctly rounded
+on every input) across an integer index, or an arctangent an ulp apart at the
+angle limit -- at most a few entries per case.  The
 image is compared where the folds agree, with a float32 summation-order
 tolerance of 1e-5 relative L2."""
 import ctypes as C
