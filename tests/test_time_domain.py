@@ -260,7 +260,7 @@ def test_torch_port_bit_identical_to_reference(name):
     np.testing.assert_array_equal(img, g[name + "_image"])
 
 
-def test_oracles_agree_up_to_atan2_ulps():
+def test_oracles_agree_up_to_torch_sqrt_rounding():
     """The numpy float32 restatement (IEEE square roots) and the torch port of
     the reference (torch's CPU float32 sqrt, an ulp off on ~0.7 % of inputs)
     agree on a 3000-trace case with the cap active except where that ulp in
