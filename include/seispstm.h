@@ -356,7 +356,8 @@ int64_t pstm_launch_count(void);
  * Problems that need more reject with PSTM_EINVAL.  The scratch holds the
  * grid-local geometry (16 B/trace), the per-tile trace lists (sized for the
  * worst case, 4 B per tile per trace) and the staged float32 trace rows;
- * storage must be PSTM_F32.  The first call on a device looks up the array's
+ * storage must be PSTM_F32.  Non-finite coordinates reject with PSTM_EINVAL, as
+ * in pstm_plan_create.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress), so make it before any stream capture.
  * All calls share the array: calls whose work overlaps on the GPU race, and
  * the array keeps the last call's contents (the error flag is cleared on every

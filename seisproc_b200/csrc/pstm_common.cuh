@@ -9,6 +9,7 @@
 #define PSTM_ERR_TIMEOUT 1
 #define PSTM_ERR_BOUNDS 2
 #define PSTM_ERR_VELOCITY 4
+#define PSTM_ERR_COORDS 8
 
 // Bounded waits on an mbarrier give up after this many nanoseconds of the
 // global timer (2 s: far beyond any legitimate wait for one pipeline stage).

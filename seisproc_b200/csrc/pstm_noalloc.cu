@@ -85,13 +85,19 @@ __device__ __forceinline__ bool noalloc_in_disc(float4 t, float cx, float cy, fl
   return (a * a + b * b < r2) && (c * c + d * d < r2);
 }
 
+// Grid-local coordinates (origin subtracted in float64).  A non-finite
+// coordinate raises PSTM_ERR_COORDS, which the entry point reports as
+// PSTM_EINVAL, as the plan path rejects such geometry.
 template <typename C>
 __global__ void noalloc_geo_kernel(const C* sx, const C* sy, const C* rx, const C* ry, int n,
-                                   double ox, double oy, float4* geo) {
+                                   double ox, double oy, float4* geo, int* err) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
-  geo[j] = make_float4((float)((double)sx[j] - ox), (float)((double)sy[j] - oy),
-                       (float)((double)rx[j] - ox), (float)((double)ry[j] - oy));
+  const float4 g = make_float4((float)((double)sx[j] - ox), (float)((double)sy[j] - oy),
+                               (float)((double)rx[j] - ox), (float)((double)ry[j] - oy));
+  if (!(isfinite(g.x) && isfinite(g.y) && isfinite(g.z) && isfinite(g.w)))
+    atomicOr(err, PSTM_ERR_COORDS);
+  geo[j] = g;
 }
 
 __global__ void __launch_bounds__(256) noalloc_count_kernel(DiscGrid g, const float4* geo, int n,
@@ -233,6 +239,8 @@ extern "C" pstm_status pstm_migrate_noalloc(const pstm_grid* grid, const pstm_pa
   p.tiles_xl = (grid->n_xl + p.shape.tile_xl - 1) / p.shape.tile_xl;
   p.n_tiles = (int64_t)p.tiles_il * p.tiles_xl;
   p.n_windows = (grid->n_times + p.shape.t_window() - 1) / p.shape.t_window();
+  if (p.n_tiles > INT32_MAX || p.n_windows > 65535)
+    return noalloc_fail(PSTM_EINVAL, "grid too large");
   p.il_dx = (float)grid->il_dx;
   p.il_dy = (float)grid->il_dy;
   p.xl_dx = (float)grid->xl_dx;
@@ -284,12 +292,12 @@ extern "C" pstm_status pstm_migrate_noalloc(const pstm_grid* grid, const pstm_pa
       noalloc_geo_kernel<double><<<nb, 256, 0, s>>>(
           (const double*)geometry->source_x, (const double*)geometry->source_y,
           (const double*)geometry->receiver_x, (const double*)geometry->receiver_y, (int)n,
-          grid->origin_x, grid->origin_y, p.geo);
+          grid->origin_x, grid->origin_y, p.geo, p.err);
     else
       noalloc_geo_kernel<float><<<nb, 256, 0, s>>>(
           (const float*)geometry->source_x, (const float*)geometry->source_y,
           (const float*)geometry->receiver_x, (const float*)geometry->receiver_y, (int)n,
-          grid->origin_x, grid->origin_y, p.geo);
+          grid->origin_x, grid->origin_y, p.geo, p.err);
     if ((st = launched("noalloc_geo_kernel")) != PSTM_OK) return st;
   }
   noalloc_count_kernel<<<(unsigned)p.n_tiles, 256, 0, s>>>(dg, p.geo, (int)n, counts);
@@ -308,10 +316,9 @@ extern "C" pstm_status pstm_migrate_noalloc(const pstm_grid* grid, const pstm_pa
   std::string why;
   if ((st = launch_velocity_check(&p, velocity, v_stride_t, v_stride_c, s, &why)) != PSTM_OK)
     return noalloc_fail(st, why);
-  if ((st = launch_forward(&p, velocity, v_stride_t, v_stride_c, image, nullptr, s, &why)) !=
+  // the fold (when asked for) is counted in the forward launch, as pstm_migrate does
+  if ((st = launch_forward(&p, velocity, v_stride_t, v_stride_c, image, fold, s, &why)) !=
       PSTM_OK)
-    return noalloc_fail(st, why);
-  if (fold && (st = launch_fold(&p, velocity, v_stride_t, v_stride_c, fold, s, &why)) != PSTM_OK)
     return noalloc_fail(st, why);
   int flags = 0;
   e = cudaMemcpyAsync(&flags, p.err, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -319,6 +326,7 @@ extern "C" pstm_status pstm_migrate_noalloc(const pstm_grid* grid, const pstm_pa
   if (e != cudaSuccess) return noalloc_fail(PSTM_ECUDA, cudaGetErrorString(e));
   if (flags & PSTM_ERR_TIMEOUT)
     return noalloc_fail(PSTM_ETIMEOUT, "a bounded device-side wait for a trace copy expired");
+  if (flags & PSTM_ERR_COORDS) return noalloc_fail(PSTM_EINVAL, "non-finite trace coordinates");
   if (flags & PSTM_ERR_VELOCITY)
     return noalloc_fail(PSTM_EINVAL,
                         "velocity must be positive and finite with V*t0 non-decreasing in t0");
