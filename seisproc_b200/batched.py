@@ -50,17 +50,34 @@ def offset_azimuth(source_x: torch.Tensor, source_y: torch.Tensor, receiver_x: t
                    receiver_y: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
     """Offset (float32, m) and source-to-receiver azimuth (degrees in [0, 360),
     clockwise from north) on the coordinates' device, in the coordinates'
-    precision as the reference forms them (models/migration_geometry.py:88-116)."""
+    precision as the reference forms them (models/migration_geometry.py:88-116):
+    dx, dy and dx^2 + dy^2 in that precision, the square root correctly
+    rounded (taken in float64 and rounded once, which equals numpy's IEEE
+    square root; torch's CPU float32 sqrt is not correctly rounded), and
+    (degrees + 360) % 360 in that precision.  The arctangent is taken in
+    float64 and rounded once: numpy's float32 arctan2 is a vectorised
+    approximation whose last bit depends on the CPU it runs on, so only a
+    trace within an ulp or two of an azimuth edge could be classed
+    differently from a given numpy build."""
     dx = receiver_x - source_x
     dy = receiver_y - source_y
-    off = torch.sqrt(dx * dx + dy * dy).to(torch.float32)
-    az = torch.remainder(torch.rad2deg(torch.atan2(dx, dy)) + 360.0, 360.0)
+    off = torch.sqrt((dx * dx + dy * dy).to(torch.float64)).to(torch.float32)
+    deg = torch.rad2deg(torch.atan2(dx.to(torch.float64), dy.to(torch.float64))).to(dx.dtype)
+    az = torch.remainder(deg + 360.0, 360.0)
     return off, az
 
 
 def bin_indices(source_x: torch.Tensor, source_y: torch.Tensor, receiver_x: torch.Tensor,
-                receiver_y: torch.Tensor, bins: Sequence[OffsetAzimuthBin]) -> List[torch.Tensor]:
+                receiver_y: torch.Tensor, bins: Sequence[OffsetAzimuthBin],
+                inclusive: bool = False) -> List[torch.Tensor]:
     """Trace indices (on the coordinates' device) of every enabled bin.
+
+    Membership is the binning table's (models/binning.py:136-158): offsets in
+    [offset_min, offset_max), azimuths in [azimuth_min, azimuth_max), wrapping
+    through north when azimuth_max < azimuth_min.  ``inclusive=True`` takes
+    MigrationGeometry.get_indices_for_bin's closed intervals instead
+    (models/migration_geometry.py:256-283), under which neighbouring bins
+    share their edges.
 
     The reference assigns traces bin by bin on the host and the worker then
     migrates bin after bin (models/binning.py:304-325,
@@ -73,6 +90,11 @@ def bin_indices(source_x: torch.Tensor, source_y: torch.Tensor, receiver_x: torc
     off, az = offset_azimuth(source_x, source_y, receiver_x, receiver_y)
 
     def member(b):
+        if inclusive:
+            ok = (off >= b.offset_min) & (off <= b.offset_max)
+            if b.azimuth_max < b.azimuth_min:
+                return ok & ((az >= b.azimuth_min) | (az <= b.azimuth_max))
+            return ok & (az >= b.azimuth_min) & (az <= b.azimuth_max)
         ok = (off >= b.offset_min) & (off < b.offset_max)
         if b.azimuth_max < b.azimuth_min:
             return ok & ((az >= b.azimuth_min) | (az < b.azimuth_max))

@@ -81,69 +81,109 @@ def survey_inputs(s: synthetic.Survey, tr):
                                s.max_angle_deg], dtype=np.float64))
 
 
-def main(ref_root: str):
+def main(ref_root: str, only=()):
+    """Regenerates every fixture, or those named in ``only``."""
     torch.set_num_threads(max(1, os.cpu_count() or 1))
     eng, kmig, cfg, vel, geo, sd = import_reference(ref_root)
     out = {}
 
+    def want(name):
+        return not only or name in only
+
     # 1. small 2D common-offset case (3 offsets x 48 CMPs x 251 samples)
     s = synthetic.survey_2d(seed=11, n_offsets=3, n_cmp=48, n_samples=251, n_diffractors=8)
     s.max_aperture_m = 400.0
-    tr, img, fold = run_engine(eng, s)
-    np.savez_compressed(os.path.join(HERE, "full_2d_small.npz"), image=img, fold=fold,
-                        **survey_inputs(s, tr), n_times=np.int64(s.n_times), tda=np.int64(0))
-    out["full_2d_small"] = float(np.abs(img).max())
+    if want("full_2d_small"):
+        tr, img, fold = run_engine(eng, s)
+        np.savez_compressed(os.path.join(HERE, "full_2d_small.npz"), image=img, fold=fold,
+                            **survey_inputs(s, tr), n_times=np.int64(s.n_times), tda=np.int64(0))
+        out["full_2d_small"] = float(np.abs(img).max())
 
     # 2. same data, time-dependent aperture, shifted time origin, fewer output samples
-    tr, img, fold = run_engine(eng, s, tda=True, n_times=200, t_min_ms=40.0)
-    inp = survey_inputs(s, tr)
-    inp["grid"][7] = 40.0
-    np.savez_compressed(os.path.join(HERE, "full_2d_tda_tmin.npz"), image=img, fold=fold, **inp,
-                        n_times=np.int64(200), tda=np.int64(1))
-    out["full_2d_tda_tmin"] = float(np.abs(img).max())
+    if want("full_2d_tda_tmin"):
+        tr, img, fold = run_engine(eng, s, tda=True, n_times=200, t_min_ms=40.0)
+        inp = survey_inputs(s, tr)
+        inp["grid"][7] = 40.0
+        np.savez_compressed(os.path.join(HERE, "full_2d_tda_tmin.npz"), image=img, fold=fold,
+                            **inp, n_times=np.int64(200), tda=np.int64(1))
+        out["full_2d_tda_tmin"] = float(np.abs(img).max())
 
     # 3. mini 3D survey, constant velocity (the reference takes a constant V only)
-    s3 = synthetic.survey_3d(n_traces=800, seed=5, n_samples=128, extent=800.0, max_offset=500.0,
-                             n_il=8, n_xl=8, spacing=25.0, n_diffractors=6, aperture=300.0,
-                             lateral_velocity=False)
-    s3.velocity_mps = 1800.0
-    tr, img, fold = run_engine(eng, s3)
-    np.savez_compressed(os.path.join(HERE, "full_3d_mini.npz"), image=img, fold=fold,
-                        **survey_inputs(s3, tr), n_times=np.int64(s3.n_times), tda=np.int64(0))
-    out["full_3d_mini"] = float(np.abs(img).max())
+    if want("full_3d_mini"):
+        s3 = synthetic.survey_3d(n_traces=800, seed=5, n_samples=128, extent=800.0,
+                                 max_offset=500.0, n_il=8, n_xl=8, spacing=25.0, n_diffractors=6,
+                                 aperture=300.0, lateral_velocity=False)
+        s3.velocity_mps = 1800.0
+        tr, img, fold = run_engine(eng, s3)
+        np.savez_compressed(os.path.join(HERE, "full_3d_mini.npz"), image=img, fold=fold,
+                            **survey_inputs(s3, tr), n_times=np.int64(s3.n_times),
+                            tda=np.int64(0))
+        out["full_3d_mini"] = float(np.abs(img).max())
 
     # 4. KirchhoffMigrator (direct DSR, no LUT) on a mini gather
-    gs = synthetic.survey_3d(n_traces=300, seed=9, n_samples=100, extent=600.0, max_offset=400.0,
-                             n_il=6, n_xl=5, spacing=30.0, n_diffractors=4, aperture=250.0,
-                             lateral_velocity=False)
-    grid = cfg.OutputGrid(n_time=90, n_inline=6, n_xline=5, dt=0.004, d_inline=30.0,
-                          d_xline=30.0, t0=0.0, x_origin=gs.origin_x, y_origin=gs.origin_y)
-    mcfg = cfg.MigrationConfig(output_grid=grid, max_aperture_m=250.0, max_angle_deg=55.0)
-    vm = vel.create_constant_velocity(1900.0)
-    mig = kmig.KirchhoffMigrator(vm, mcfg, device=torch.device("cpu"), use_traveltime_lut=False)
-    gtr = gs.traces.cpu().numpy().astype(np.float32)
-    gather = sd.SeismicData(traces=gtr, sample_rate=4.0)
-    geom = geo.MigrationGeometry(source_x=gs.source_x, source_y=gs.source_y,
-                                 receiver_x=gs.receiver_x, receiver_y=gs.receiver_y)
-    mimg, mfold = mig.migrate_gather(gather, geom)
-    np.savez_compressed(os.path.join(HERE, "migrator_mini.npz"), image=mimg.numpy(),
-                        fold=mfold.numpy(), traces=gtr,
-                        source_x=geom.source_x, source_y=geom.source_y,
-                        receiver_x=geom.receiver_x, receiver_y=geom.receiver_y,
-                        grid=np.array([gs.origin_x, gs.origin_y, 30.0, 30.0, 6, 5, 4.0, 0.0,
-                                       1900.0, 250.0, 55.0, 90, 0.004], dtype=np.float64))
-    out["migrator_mini"] = float(mimg.abs().max())
+    if want("migrator_mini"):
+        gs = synthetic.survey_3d(n_traces=300, seed=9, n_samples=100, extent=600.0,
+                                 max_offset=400.0, n_il=6, n_xl=5, spacing=30.0, n_diffractors=4,
+                                 aperture=250.0, lateral_velocity=False)
+        grid = cfg.OutputGrid(n_time=90, n_inline=6, n_xline=5, dt=0.004, d_inline=30.0,
+                              d_xline=30.0, t0=0.0, x_origin=gs.origin_x, y_origin=gs.origin_y)
+        mcfg = cfg.MigrationConfig(output_grid=grid, max_aperture_m=250.0, max_angle_deg=55.0)
+        vm = vel.create_constant_velocity(1900.0)
+        mig = kmig.KirchhoffMigrator(vm, mcfg, device=torch.device("cpu"),
+                                     use_traveltime_lut=False)
+        gtr = gs.traces.cpu().numpy().astype(np.float32)
+        gather = sd.SeismicData(traces=gtr, sample_rate=4.0)
+        geom = geo.MigrationGeometry(source_x=gs.source_x, source_y=gs.source_y,
+                                     receiver_x=gs.receiver_x, receiver_y=gs.receiver_y)
+        mimg, mfold = mig.migrate_gather(gather, geom)
+        np.savez_compressed(os.path.join(HERE, "migrator_mini.npz"), image=mimg.numpy(),
+                            fold=mfold.numpy(), traces=gtr,
+                            source_x=geom.source_x, source_y=geom.source_y,
+                            receiver_x=geom.receiver_x, receiver_y=geom.receiver_y,
+                            grid=np.array([gs.origin_x, gs.origin_y, 30.0, 30.0, 6, 5, 4.0, 0.0,
+                                           1900.0, 250.0, 55.0, 90, 0.004], dtype=np.float64))
+        out["migrator_mini"] = float(mimg.abs().max())
 
     # 5. the full-size 2D workload: outputs + SHA-256 of the regenerated input
-    s2 = synthetic.survey_2d(seed=1234)
-    tr, img, fold = run_engine(eng, s2)
-    np.savez_compressed(os.path.join(HERE, "full_2d_config.npz"), image=img, fold=fold,
-                        input_sha256=np.array(sha_f32(tr)),
-                        geom_sha256=np.array(sha_f32(np.stack([s2.source_x, s2.source_y,
-                                                               s2.receiver_x, s2.receiver_y]))))
-    out["full_2d_config"] = float(np.abs(img).max())
+    if want("full_2d_config"):
+        s2 = synthetic.survey_2d(seed=1234)
+        tr, img, fold = run_engine(eng, s2)
+        np.savez_compressed(os.path.join(HERE, "full_2d_config.npz"), image=img, fold=fold,
+                            input_sha256=np.array(sha_f32(tr)),
+                            geom_sha256=np.array(sha_f32(np.stack([s2.source_x, s2.source_y,
+                                                                   s2.receiver_x,
+                                                                   s2.receiver_y]))))
+        out["full_2d_config"] = float(np.abs(img).max())
+
+    # 6. a larger 3D survey at full trace density around the grid: 20k traces x
+    # 500 samples -> 16 x 16 x 500 at 25 m, 800 m aperture, constant V (the
+    # reference takes a constant V only); outputs + SHA-256 of the regenerated
+    # input (generated on the CPU, as the test regenerates it)
+    if want("full_3d_20k"):
+        s6 = survey_3d_20k()
+        tr, img, fold = run_engine(eng, s6)
+        np.savez_compressed(os.path.join(HERE, "full_3d_20k.npz"), image=img, fold=fold,
+                            input_sha256=np.array(sha_f32(tr)),
+                            geom_sha256=np.array(sha_f32(np.stack([s6.source_x, s6.source_y,
+                                                                   s6.receiver_x,
+                                                                   s6.receiver_y]))),
+                            velocity_mps=np.float64(s6.velocity_mps))
+        out["full_3d_20k"] = float(np.abs(img).max())
     print(out)
 
 
+def survey_3d_20k() -> synthetic.Survey:
+    """The full_3d_20k fixture's input (CPU generator, seed 31)."""
+    s = synthetic.survey_3d(n_traces=20000, seed=31, n_samples=500, extent=2400.0,
+                            max_offset=1500.0, n_il=16, n_xl=16, spacing=25.0, n_diffractors=24,
+                            aperture=800.0, lateral_velocity=False)
+    s.velocity_mps = 2200.0
+    return s
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SEISPROC_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <path to the SeisProc checkout> "
+                 "[fixture ...] (or set SEISPROC_REFERENCE)")
+    main(ref, tuple(sys.argv[2:]))

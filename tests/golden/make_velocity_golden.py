@@ -102,4 +102,8 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SEISPROC_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <path to the SeisProc checkout> "
+                 "(or set SEISPROC_REFERENCE)")
+    main(ref)

@@ -73,3 +73,49 @@ def test_invalid_bins_rejected():
         OffsetAzimuthBin("bad", 100.0, 50.0)
     with pytest.raises(ValueError):
         OffsetAzimuthBin("bad", 0.0, 50.0, 0.0, 400.0)
+
+
+# --- pinned to the reference's own binning (tests/golden/make_binning_golden.py) ---
+
+def _golden_bins(d, table):
+    rows = d[f"{table}_bins"]
+    return [OffsetAzimuthBin(f"{table}{i}", float(r[0]), float(r[1]), float(r[2]), float(r[3]),
+                             enabled=bool(r[4])) for i, r in enumerate(rows)]
+
+
+def _split(d, key):
+    counts = d[key.replace("indices", "counts")]
+    return np.split(d[key], np.cumsum(counts)[:-1])
+
+
+@pytest.mark.parametrize("table", ["ovt", "narrow", "common_offset"])
+def test_classes_match_reference_binning_table(table):
+    """bin_indices reproduces BinningTable.assign_traces_batch on float32
+    geometry, edge traces included, index for index.  Offsets equal the
+    reference's bit for bit; azimuths may differ in the last bits (numpy's
+    float32 arctan2 is not correctly rounded) without moving any trace across
+    a bin edge."""
+    from conftest import load_golden
+    d = load_golden("binning")
+    g = [torch.from_numpy(d[k]) for k in ("source_x", "source_y", "receiver_x", "receiver_y")]
+    off, az = offset_azimuth(*g)
+    assert np.array_equal(off.numpy(), d["offset"])
+    assert float(np.abs(az.numpy() - d["azimuth"]).max()) < 1e-4
+    got = bin_indices(*g, _golden_bins(d, table))
+    want = _split(d, f"{table}_indices")
+    assert len(got) == len(want)
+    for a, b in zip(got, want):
+        assert np.array_equal(np.sort(a.numpy()), b)
+
+
+def test_closed_intervals_match_reference_get_indices_for_bin():
+    """inclusive=True reproduces MigrationGeometry.get_indices_for_bin, whose
+    closed intervals put edge traces in both neighbouring bins."""
+    from conftest import load_golden
+    d = load_golden("binning")
+    g = [torch.from_numpy(d[k]) for k in ("source_x", "source_y", "receiver_x", "receiver_y")]
+    got = bin_indices(*g, _golden_bins(d, "ovt"), inclusive=True)
+    want = _split(d, "ovt_closed_indices")
+    assert sum(w.size for w in want) > sum(np.diff(np.r_[0, np.cumsum(d["ovt_counts"])]))
+    for a, b in zip(got, want):
+        assert np.array_equal(np.sort(a.numpy()), b)

@@ -67,7 +67,21 @@ def test_velocity_reference_arm_and_unavailable_configs():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["metric"] == "V_rms grid Gsamples/s"
     assert d["value"] > 0 and "RegularGridInterpolator" in d["cpu_baseline"]["sample"]
-    for cfg in ("lsq", "batched"):
-        d = json.loads(_run(["--config", cfg, "--impl", "reference"])[0])
-        assert d["impl"] == "reference" and d["unavailable"]
+    d = json.loads(_run(["--config", "lsq", "--impl", "reference"])[0])
+    assert d["impl"] == "reference" and d["unavailable"]
     assert _run(["--config", "lsq", "--impl", "reference"], env={"RANK": "1"}) == []
+
+
+def test_batched_reference_arm_json_line():
+    """The batched config's reference arm: the reference algorithm migrating the
+    classes one bin at a time on a crop, same metric as the GPU arm."""
+    lines = _run(["--config", "batched", "--impl", "reference", "--steps", "1", "--warmup",
+                  "0", "--classes", "3", "--samples", "100", "--grid", "20", "--crop", "2"])
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0
+    assert d["metric"] == "PSTM Gpairs/s (out-sample x trace), batched classes"
+    assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert d["config"]["workload"].startswith("batched 3D PSTM: 3 offset/azimuth classes")
+    assert _run(["--config", "batched", "--impl", "reference", "--classes", "2"],
+                env={"RANK": "1"}) == []

@@ -84,6 +84,48 @@ def test_full_2d_config_port_matches_reference():
     assert np.array_equal(fold.numpy(), ref["fold"])
 
 
+def _survey_3d_20k():
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import survey_3d_20k
+    return survey_3d_20k()
+
+
+# columns of the 16 x 16 grid checked on the CPU: corners, edges, interior
+_COLS_20K = np.array([0, 7, 15, 17, 40, 68, 102, 119, 120, 135, 153, 187, 204, 240, 247, 255])
+
+
+def test_full_3d_20k_port_matches_reference_on_columns():
+    """The 20k-trace 3D fixture (the reference's migrate_bin_full at constant V),
+    regenerated from its seed, checked on 16 of its 256 columns: the port
+    within 1e-6 with the same fold (bit-exactness needs the reference's own
+    100-point tiles, whose trace sets fix the summation order) and the FP64
+    oracle within 2e-5 with the fold within 1e-5 of the pairs."""
+    ref = load_golden("full_3d_20k")
+    s = _survey_3d_20k()
+    tr = s.traces.numpy()
+    assert hashlib.sha256(tr.astype(np.float32).tobytes()).hexdigest() == str(ref["input_sha256"])
+    assert float(ref["velocity_mps"]) == s.velocity_mps
+    torch.set_num_threads(4)
+    img, fold = P.engine_full_port(tr, s.source_x, s.source_y, s.receiver_x, s.receiver_y,
+                                   s.origin_x, s.origin_y, s.il_spacing, s.xl_spacing, s.n_il,
+                                   s.n_xl, s.dt_ms, s.t_min_ms, s.n_times, s.velocity_mps,
+                                   s.max_aperture_m, s.max_angle_deg, column_subset=_COLS_20K)
+    ri = ref["image"].reshape(s.n_times, -1)[:, _COLS_20K]
+    rf = ref["fold"].reshape(s.n_times, -1)[:, _COLS_20K]
+    assert rel_l2(img.numpy().reshape(s.n_times, -1)[:, _COLS_20K], ri) < 1e-6
+    assert np.array_equal(fold.numpy().reshape(s.n_times, -1)[:, _COLS_20K], rf)
+    il, xl = _COLS_20K // s.n_xl, _COLS_20K % s.n_xl
+    cx = (s.origin_x + il * s.il_spacing).astype(np.float32)
+    cy = (s.origin_y + xl * s.xl_spacing).astype(np.float32)
+    t_ms = (np.arange(s.n_times, dtype=np.float32) * np.float32(s.dt_ms)).astype(np.float64)
+    oi, of = O.migrate_fp64(tr, s.source_x, s.source_y, s.receiver_x, s.receiver_y, cx, cy, t_ms,
+                            s.velocity_mps, s.dt_ms, 0.0, s.max_aperture_m, s.max_angle_deg)
+    assert rel_l2(oi, ri) < 2e-5
+    assert np.abs(of - rf).sum() <= max(2, 1e-5 * rf.sum())
+
+
 # --- known answers restated from the reference's tests -----------------------
 
 def _one_trace(h_s, h_r, z_m, v, n_s=2048, dt=1.0, weight="none", ramp=True):
