@@ -14,7 +14,9 @@ aperture, 60 deg angle.  Synthetic, seeded.
 ``--antialias --utm --storage bf16|f16`` is the anti-aliased workload with
 traces stored in 16 bits and world coordinates offset by a UTM origin.  Every
 run quotes ``error_vs_fp64``: the rel-L2 of its image against the FP64 oracle on
-a small centred crop of columns (``--err-crop``).
+64 columns spread over the grid (2 x 2 clusters at the corners, the edge
+midpoints, the centre and seeded interior positions; ``--err-clusters``), and
+the fold mismatch as a fraction of the pairs checked.
 
 One JSON line on rank 0.  ``value`` = pairs / device time of one step with the
 inputs resident in HBM (stage traces, then forward migration with the fold; the geometry
@@ -179,6 +181,78 @@ def cpu_crop_columns(s, side: int):
     return np.sort((il * s.n_xl + xl).ravel())
 
 
+def error_clusters(n_il: int, n_xl: int, n_clusters: int = 16, seed: int = 11):
+    """2 x 2 column clusters checked against the FP64 oracle: the four corners,
+    the four edge midpoints, the centre, and seeded random interior clusters
+    (16 clusters = 64 columns by default).  Returns a list of flat column
+    index arrays (il * n_xl + xl)."""
+    a_il, a_xl = max(n_il - 2, 0), max(n_xl - 2, 0)
+    anchors = [(0, 0), (0, a_xl), (a_il, 0), (a_il, a_xl),
+               (0, a_xl // 2), (a_il // 2, 0), (a_il, a_xl // 2), (a_il // 2, a_xl),
+               (a_il // 2, a_xl // 2)]
+    rs = np.random.RandomState(seed)
+    while len(anchors) < n_clusters:
+        anchors.append((int(rs.randint(1, max(a_il, 2))), int(rs.randint(1, max(a_xl, 2)))))
+    out = []
+    for i0, j0 in anchors[:n_clusters]:
+        il = np.arange(i0, min(i0 + 2, n_il))[:, None]
+        xl = np.arange(j0, min(j0 + 2, n_xl))[None, :]
+        out.append(np.sort((il * n_xl + xl).ravel()))
+    return out
+
+
+def fp64_check(s, img_cols, fold_cols, clusters, antialias: bool, l_max: float, storage: str,
+               threads: int = 0):
+    """rel-L2 of the image columns against the FP64 oracle over all clusters
+    (one oracle run per cluster with the traces in its aperture, in a thread
+    pool), and the fold mismatch as a count and a fraction of the pairs."""
+    import concurrent.futures as cf
+    dev = img_cols.device
+    todo = []
+    for cols in clusters:
+        e = torch.from_numpy(cols).to(dev)
+        todo.append((cols, img_cols[:, e].double().cpu().numpy(),
+                     fold_cols[:, e].double().cpu().numpy()))
+    n_thr = threads or min(len(todo), max(1, len(os.sched_getaffinity(0))))
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=n_thr) as ex:
+        res = list(ex.map(lambda c: run_fp64_crop(s, c[0], antialias, l_max), todo))
+    wall = time.perf_counter() - t0
+    num = den = mism = pairs = 0.0
+    worst = 0.0
+    n_tr = 0
+    for (cols, gi, gf), (oi, of, _, ntr) in zip(todo, res):
+        num += float(np.sum((gi - oi) ** 2))
+        d = float(np.sum(oi ** 2))
+        den += d
+        worst = max(worst, float(np.linalg.norm(gi - oi) / max(np.sqrt(d), 1e-300)))
+        mism += float(np.abs(gf - of).sum())
+        pairs += float(of.sum())
+        n_tr += ntr
+    return {"rel_l2": float(np.sqrt(num / max(den, 1e-300))), "worst_cluster_rel_l2": worst,
+            "fold_mismatch": mism, "fold_mismatch_frac": mism / max(pairs, 1.0),
+            "pairs_checked": pairs, "columns": int(sum(c.size for c in clusters)),
+            "clusters": "2x2 columns at the 4 corners, 4 edge midpoints, the centre and "
+                        f"{max(len(clusters) - 9, 0)} seeded interior positions",
+            "traces_in_apertures": n_tr, "oracle_wall_s": wall, "oracle_threads": n_thr,
+            "oracle": "FP64 restatement" + (" with anti-alias" if antialias else ""),
+            "storage": storage, "sum_sq_err": num, "sum_sq_ref": den}
+
+
+def merge_checks(checks, storage: str):
+    """One error summary over several fp64_check results (e.g. several classes)."""
+    num = sum(c["sum_sq_err"] for c in checks)
+    den = sum(c["sum_sq_ref"] for c in checks)
+    mism = sum(c["fold_mismatch"] for c in checks)
+    pairs = sum(c["pairs_checked"] for c in checks)
+    return {"rel_l2": float(np.sqrt(num / max(den, 1e-300))),
+            "worst_cluster_rel_l2": max(c["worst_cluster_rel_l2"] for c in checks),
+            "fold_mismatch": mism, "fold_mismatch_frac": mism / max(pairs, 1.0),
+            "pairs_checked": pairs, "columns": sum(c["columns"] for c in checks),
+            "oracle_wall_s": sum(c["oracle_wall_s"] for c in checks),
+            "oracle": checks[0]["oracle"], "storage": storage}
+
+
 def run_cpu_port(s, cols, fold_pairs_cols):
     """Reference-port CPU timing on a column crop (all traces supplied)."""
     from oracle.ref_port import engine_full_port
@@ -265,15 +339,22 @@ def bench_ours(args):
     vel = torch.from_numpy(s.vrms.reshape(n_t, -1)).to(dev)
     coords = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
               for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    plan_kw = dict(n_il=s.n_il, n_xl=s.n_xl, n_times=n_t, origin_x=s.origin_x,
+                   origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                   xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                   in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                   max_angle_deg=s.max_angle_deg, storage=args.storage,
+                   antialias=args.antialias, aa_dx=s.il_spacing, aa_dy=s.xl_spacing,
+                   aa_max_halfwidth=args.aa_lmax, forward_only=True)
     torch.cuda.synchronize()
+    t_tune = time.perf_counter()
+    variant = args.variant
+    if variant == "auto":
+        from seisproc_b200 import autotune
+        variant = autotune.choose_variant(coords, velocity=vel, **plan_kw)
+    t_tune = time.perf_counter() - t_tune
     t_plan = time.perf_counter()
-    plan = PSTMPlan(*coords, n_il=s.n_il, n_xl=s.n_xl, n_times=n_t, origin_x=s.origin_x,
-                    origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
-                    xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
-                    in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
-                    max_angle_deg=s.max_angle_deg, storage=args.storage, variant=args.variant,
-                    antialias=args.antialias, aa_dx=s.il_spacing, aa_dy=s.xl_spacing,
-                    aa_max_halfwidth=args.aa_lmax, forward_only=True)
+    plan = PSTMPlan(*coords, variant=variant, **plan_kw)
     torch.cuda.synchronize()
     t_plan = time.perf_counter() - t_plan
     traces = s.traces
@@ -430,20 +511,17 @@ def bench_ours(args):
         if world == 1 and not args.no_cpu:
             img_cols = image.reshape(n_t, -1)
             fold_cols_t = f.reshape(n_t, -1)
-            # error of this result against the FP64 oracle on a small crop
-            ecols = cpu_crop_columns(s, args.err_crop)
-            eidx = torch.from_numpy(ecols).to(dev)
-            oi, of, o_sec, o_tr = run_fp64_crop(s, ecols, args.antialias, args.aa_lmax)
-            gi = img_cols[:, eidx].double().cpu().numpy()
-            gf = fold_cols_t[:, eidx].double().cpu().numpy()
-            err = {"rel_l2": float(np.linalg.norm(gi - oi) / max(np.linalg.norm(oi), 1e-300)),
-                   "fold_mismatch": float(np.abs(gf - of).sum()),
-                   "columns": int(ecols.size), "traces_in_crop": o_tr,
-                   "oracle": "FP64 restatement" + (" with anti-alias" if args.antialias else ""),
-                   "storage": args.storage}
+            # error of this result against the FP64 oracle on columns spread over the grid
+            err = fp64_check(s, img_cols, fold_cols_t,
+                             error_clusters(s.n_il, s.n_xl, args.err_clusters),
+                             args.antialias, args.aa_lmax, args.storage)
             if args.antialias:
                 # the reference has no anti-aliased migration: the FP64 oracle
-                # run above is the CPU baseline
+                # on a centred crop is the CPU baseline
+                ecols = cpu_crop_columns(s, args.err_crop)
+                eidx = torch.from_numpy(ecols).to(dev)
+                oi, of, o_sec, o_tr = run_fp64_crop(s, ecols, args.antialias, args.aa_lmax)
+                gf = fold_cols_t[:, eidx].double().cpu().numpy()
                 pc = float(gf.sum())
                 cb = {"value": pc / o_sec / 1e9, "unit": "Gpairs/s", "cores": 1, "kind": "port",
                       "sample": f"centred {args.err_crop}x{args.err_crop}-column crop x {n_t} "
@@ -465,8 +543,12 @@ def bench_ours(args):
                        "antialias": bool(args.antialias),
                        "traces_per_gpu": s.n_traces, "pairs_per_step_per_gpu": pairs,
                        "plan": plan.stats(), "plan_build_s": t_plan, "datagen_s": t_gen,
+                       "shape_choice": ("autotuner (cached per problem class; this run's "
+                                        f"choice took {t_tune:.2f} s)"
+                                        if args.variant == "auto" else "fixed --variant"),
                        "l2": "inputs (traces) larger than L2; no flush",
-                       "parallelism": f"output-survey shards, {world} rank(s), no collective"},
+                       "parallelism": (f"replicas: one independent survey per rank, {world} rank(s), "
+                                       "no collective") if world > 1 else "one GPU"},
             "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clocks, "error_vs_fp64": err,
         }
@@ -478,34 +560,173 @@ def bench_ours(args):
     return result
 
 
-def bench_batched(args):
-    """64 offset/azimuth classes (trace counts log-uniform 2k-40k), one persistent
-    launch per step replayed from a CUDA graph; value = pairs of all classes / time."""
-    from seisproc_b200 import _lib, synthetic
-    from seisproc_b200.batched import BatchedPSTM
+def batched_surveys(args, dev):
+    """The batched workload: the first ``args.classes`` of 64 offset/azimuth
+    classes (8 offset bins x 8 azimuth sectors, trace counts log-uniform
+    2k-40k, seed 64), one synthetic survey per class sharing diffractors,
+    velocity and grid."""
+    from seisproc_b200 import synthetic
+    counts = synthetic.class_counts_loguniform(64, 2000, 40000, seed=64)[:args.classes]
+    return synthetic.survey_classes(counts, seed=64, device=dev, n_samples=args.samples,
+                                    n_il=args.grid, n_xl=args.grid)
+
+
+def class_plans(surveys, storage: str, variant, dev, vel):
+    """One forward_only plan per class; ``variant="auto"`` takes each class's
+    kernel shape from the autotuner (cached per problem class)."""
+    from seisproc_b200 import autotune
     from seisproc_b200.kirchhoff import PSTMPlan
-    torch.cuda.set_device(0)
-    dev = torch.device("cuda", 0)
-    L = _lib.lib()
-    counts = synthetic.class_counts_loguniform(64, 2000, 40000, seed=64)
-    t_gen = time.perf_counter()
-    surveys = synthetic.survey_classes(counts, seed=64, device=dev, n_samples=args.samples,
-                                       n_il=args.grid, n_xl=args.grid)
-    torch.cuda.synchronize()
-    t_gen = time.perf_counter() - t_gen
-    s0 = surveys[0]
     plans = []
     for s in surveys:
         c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
              for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
-        plans.append(PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times,
-                              origin_x=s.origin_x, origin_y=s.origin_y, il_dx=s.il_spacing,
-                              il_dy=0.0, xl_dx=0.0, xl_dy=s.xl_spacing, t0_ms=0.0,
-                              dt_ms=s.dt_ms, n_samples=s.n_samples, in_t0_ms=0.0,
-                              in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
-                              max_angle_deg=s.max_angle_deg, storage=args.storage,
-                              variant=args.variant))
+        kw = dict(n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+                  origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                  xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                  in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                  max_angle_deg=s.max_angle_deg, storage=storage, forward_only=True)
+        v = autotune.choose_variant(c, velocity=vel, **kw) if variant == "auto" else variant
+        plans.append(PSTMPlan(*c, variant=v, **kw))
+    return plans
+
+
+def checked_classes(pairs_per_class, n: int = 8, seed: int = 8):
+    """Classes checked against the FP64 oracle: the four with the most pairs and
+    seeded others among those with pairs."""
+    live = [i for i, p in enumerate(pairs_per_class) if p > 0]
+    top = sorted(live, key=lambda i: -pairs_per_class[i])[:4]
+    rest = [i for i in live if i not in top]
+    rs = np.random.RandomState(seed)
+    extra = list(rs.choice(rest, size=min(n - len(top), len(rest)), replace=False)) if rest else []
+    return sorted(top + [int(i) for i in extra])
+
+
+def shard_partition(s, world: int):
+    """The sharded mode's partition of one survey: inline slabs (sizes
+    differing by at most one) and, per slab, the traces whose two legs reach
+    it within the aperture (its halo)."""
+    from seisproc_b200 import sharding as S
+    slabs = S.inline_slabs(s.n_il, world)
+    halos = []
+    for il0, il1 in slabs:
+        box = S.slab_bbox(s.origin_x, s.origin_y, s.il_spacing, 0.0, 0.0, s.xl_spacing, s.n_xl,
+                          il0, il1)
+        halos.append(S.halo_traces(s.source_x, s.source_y, s.receiver_x, s.receiver_y, box,
+                                   s.max_aperture_m))
+    return slabs, halos
+
+
+def shard_aggregate(ms: float, pairs: float, device, group=None):
+    """Whole-job figures from one rank's timed milliseconds and pairs: the
+    slowest rank's time and the pairs of all ranks (every rank calls it)."""
+    import torch.distributed as dist
+    t = torch.tensor([ms, pairs], dtype=torch.float64, device=device)
+    if dist.is_initialized():
+        m = t[:1].clone()
+        dist.all_reduce(m, op=dist.ReduceOp.MAX, group=group)
+        p_ = t[1:].clone()
+        dist.all_reduce(p_, op=dist.ReduceOp.SUM, group=group)
+        return float(m.item()), float(p_.item())
+    return ms, pairs
+
+
+def bench_sharded(args):
+    """N ranks (one per GPU) migrate ONE survey: rank r owns inline slab r of
+    the output grid and migrates it from its halo traces (strong scaling; the
+    step has no collective).  After the timed steps the slabs are gathered to
+    every rank once and rank 0 checks the stitched image's fold against a
+    one-plan migration of its own slab's columns."""
+    import datetime
+    import torch.distributed as dist
+    from seisproc_b200 import _lib
+    from seisproc_b200.sharding import ShardedPSTM
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    L = _lib.lib()
+    s = make_workload(dev, 0, args)  # the same survey on every rank
+    torch.cuda.synchronize()
+    sh = ShardedPSTM(s.source_x, s.source_y, s.receiver_x, s.receiver_y, n_il=s.n_il,
+                     n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x, origin_y=s.origin_y,
+                     il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0, xl_dy=s.xl_spacing, t0_ms=0.0,
+                     dt_ms=s.dt_ms, n_samples=s.n_samples, in_t0_ms=0.0, in_dt_ms=s.dt_ms,
+                     max_aperture_m=s.max_aperture_m, max_angle_deg=s.max_angle_deg,
+                     velocity=torch.from_numpy(s.vrms), storage=args.storage, forward_only=True,
+                     device=dev)
+    local_tr = sh.local_traces(s.traces)
+    img = fold = None
+    for _ in range(args.warmup):
+        sh.plan.load_traces(local_tr)
+        img, fold = sh.plan.migrate_loaded(sh.velocity)
+    sh.plan.check()
+    pairs_local = float(fold[:, :sh.local_il].double().sum())
+    dist.barrier()
+    torch.cuda.synchronize()
+    l0 = L.pstm_launch_count()
+    with ClockSampler(local) as clk:
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            sh.plan.load_traces(local_tr)
+            sh.plan.migrate_loaded(sh.velocity, image=img, fold=fold)
+        e.record()
+        torch.cuda.synchronize()
+    launches = L.pstm_launch_count() - l0
+    dist.barrier()
+    ms, pairs_all = shard_aggregate(a.elapsed_time(e) / args.steps, pairs_local, dev)
+    whole_fold = sh.gather(fold[:, :sh.local_il].contiguous())
+    ok = bool(float(whole_fold.double().sum()) == pairs_all)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "PSTM Gpairs/s (out-sample x trace)",
+            "value": pairs_all / (ms * 1e-3) / 1e9, "unit": "Gpairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": args.storage, "data": "synthetic",
+            "config": {"workload": workload_name(args), "storage": args.storage,
+                       "pairs_per_step": pairs_all,
+                       "parallelism": f"inline slabs over {world} ranks: one survey, halo "
+                                      "traces per slab, no collective in the step, slabs "
+                                      "gathered once after timing",
+                       "slab_inlines": [b - a_ for a_, b in sh.slabs],
+                       "halo_traces_rank0": int(sh.halo.size),
+                       "gathered_fold_matches_pairs": ok,
+                       "l2": "inputs larger than L2; no flush"},
+            "gpu_launches": int(launches * world), "clocks": clk.summary()}), flush=True)
+    sh.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def bench_batched(args):
+    """64 offset/azimuth classes (trace counts log-uniform 2k-40k), one persistent
+    launch per step replayed from a CUDA graph; value = pairs of all classes / time.
+
+    The line also carries the batched kernel's roofline (pairs / its CUDA-event
+    time), ``error_vs_fp64`` of the run's storage and of the two others on
+    checked classes, the reference port per class on a crop as the CPU baseline,
+    and ``e2e``: every class from page-locked host buffers through
+    ``MigrationEngine.migrate_bins_full`` into page-locked host images."""
+    from seisproc_b200 import _lib
+    from seisproc_b200.batched import BatchedPSTM
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    L = _lib.lib()
+    t_gen = time.perf_counter()
+    surveys = batched_surveys(args, dev)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_gen
+    s0 = surveys[0]
+    n_t = s0.n_times
     vel = torch.from_numpy(s0.vrms).to(dev)
+    t_tune = time.perf_counter()
+    plans = class_plans(surveys, args.storage, args.variant, dev, vel)
+    torch.cuda.synchronize()
+    t_tune = time.perf_counter() - t_tune
     bufs = [s.traces for s in surveys]
     b = BatchedPSTM(plans, vel)
     b.capture(bufs)
@@ -513,7 +734,8 @@ def bench_batched(args):
         b.replay()
     torch.cuda.synchronize()
     b.check()
-    pairs = float(sum(f.double().sum() for f in b.folds))
+    pairs_c = [float(f.double().sum()) for f in b.folds]
+    pairs = float(sum(pairs_c))
     l0 = L.pstm_launch_count()
     with ClockSampler(0) as clk:
         a = torch.cuda.Event(enable_timing=True)
@@ -525,23 +747,185 @@ def bench_batched(args):
         torch.cuda.synchronize()
     b.check()
     ms = a.elapsed_time(e) / args.steps
-    n_tr = int(sum(s.n_traces for s in surveys))
-    res = {"metric": "PSTM Gpairs/s (out-sample x trace), batched classes", "value":
-           pairs / (ms * 1e-3) / 1e9, "unit": "Gpairs/s", "n_gpus": 1, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
-           "config": {"workload": f"batched 3D PSTM: 64 offset/azimuth classes, {n_tr} traces "
-                                  f"x {args.samples} samples, per-class "
+    launches = b.launches_per_replay * args.steps
+    # the batched kernel alone (traces already staged): velocity check + persistent launch
+    kms = []
+    for _ in range(3):
+        a.record()
+        b.migrate()
+        e.record()
+        torch.cuda.synchronize()
+        kms.append(a.elapsed_time(e))
+    kernel_ms = statistics.median(kms)
+    pk = peaks()
+    peak_pairs = 148 * MUFU_PER_SM_CLK / RSQRT_PER_PAIR * pk["sm_max_mhz"] * 1e6 / 1e12
+    achieved = pairs / (kernel_ms * 1e-3) / 1e12
+    roof = {"bound": "mufu", "achieved": achieved, "peak": peak_pairs, "unit": "Tpairs/s",
+            "frac": achieved / peak_pairs, "traffic": None, "mufu_per_pair": RSQRT_PER_PAIR,
+            "traffic_note": "not captured for the batched launch",
+            "peak_source": f"{pk['source']} sm_max_mhz {pk['sm_max_mhz']}",
+            "kernel": "pstm_batch_kernel (persistent, all classes, fold counted in the launch)",
+            "kernel_ms": kernel_ms}
+    err, cb, e2e = None, None, None
+    if not args.no_cpu:
+        clusters = error_clusters(surveys[0].n_il, surveys[0].n_xl, args.err_clusters)
+        chk = checked_classes(pairs_c)
+
+        def check_images(images, folds, storage):
+            return merge_checks([fp64_check(surveys[i], images[q].reshape(n_t, -1),
+                                            folds[q].reshape(n_t, -1), clusters, False,
+                                            args.aa_lmax, storage)
+                                 for q, i in enumerate(chk)], storage)
+
+        err = {args.storage: check_images([b.images[i] for i in chk], [b.folds[i] for i in chk],
+                                          args.storage)}
+        for st in ("f32", "bf16", "f16"):
+            if st == args.storage:
+                continue
+            sub = class_plans([surveys[i] for i in chk], st, args.variant, dev, vel)
+            bs = BatchedPSTM(sub, vel)
+            bs.load([surveys[i].traces for i in chk])
+            bs.migrate()
+            torch.cuda.synchronize()
+            bs.check()
+            err[st] = check_images(bs.images, bs.folds, st)
+            bs.close()
+            for p_ in sub:
+                p_.close()
+        err["classes_checked"] = chk
+        err["clusters_per_class"] = len(clusters)
+        # CPU baseline: the reference port on a centred crop of every class
+        cols = cpu_crop_columns(surveys[0], args.crop)
+        ecol = torch.from_numpy(cols).to(dev)
+        cp, csec, ncls = 0.0, 0.0, 0
+        for i, sv in enumerate(surveys):
+            pc = float(b.folds[i].reshape(n_t, -1)[:, ecol].double().sum())
+            if pc <= 0:
+                continue
+            r = run_cpu_port(sv, cols, pc)
+            cp += pc
+            csec += r["seconds"]
+            ncls += 1
+        cb = {"value": cp / max(csec, 1e-12) / 1e9, "unit": "Gpairs/s",
+              "cores": len(os.sched_getaffinity(0)), "kind": "port",
+              "sample": f"every class with pairs in a centred {args.crop}x{args.crop}-column crop "
+                        f"({ncls} classes, one bin at a time as the reference worker runs "
+                        f"them), all of each class's traces supplied, {cp:.3e} pairs; constant "
+                        "V = mean V_rms"}
+    if not args.no_e2e:
+        from seisproc_b200.engine import MigrationEngine
+        host_bins = []
+        for sv in surveys:
+            t = torch.empty(tuple(sv.traces.shape), dtype=torch.float32, pin_memory=True)
+            t.copy_(sv.traces)
+            hb = {"traces": t.numpy()}
+            for key in ("source_x", "source_y", "receiver_x", "receiver_y"):
+                h = torch.empty(getattr(sv, key).shape, dtype=torch.float64, pin_memory=True)
+                h.copy_(torch.from_numpy(getattr(sv, key)))
+                hb[key] = h.numpy()
+            host_bins.append(hb)
+        host_v = torch.empty(s0.vrms.shape, dtype=torch.float32, pin_memory=True)
+        host_v.copy_(torch.from_numpy(s0.vrms))
+        shape = (n_t, s0.n_il, s0.n_xl)
+        try:
+            outs = [(torch.empty(shape, pin_memory=True), torch.empty(shape, pin_memory=True))
+                    for _ in surveys]
+            out_kind = "page-locked tensors"
+        except RuntimeError:
+            outs = [(np.empty(shape, np.float32), np.empty(shape, np.float32)) for _ in surveys]
+            out_kind = "numpy arrays (page-locking the outputs failed)"
+        eng = MigrationEngine(storage=args.storage, variant=args.variant)
+        kw = dict(origin_x=s0.origin_x, origin_y=s0.origin_y, il_spacing=s0.il_spacing,
+                  xl_spacing=s0.xl_spacing, azimuth_deg=0.0, n_il=s0.n_il, n_xl=s0.n_xl,
+                  dt_ms=s0.dt_ms, t_min_ms=0.0, n_times=n_t, max_aperture_m=s0.max_aperture_m,
+                  max_angle_deg=s0.max_angle_deg, normalize=True, velocity_model=host_v.numpy(),
+                  out=outs)
+        eng.migrate_bins_full(host_bins, **kw)
+        calls = []
+        for _ in range(max(2, min(args.steps, 3))):
+            a.record()
+            eng.migrate_bins_full(host_bins, **kw)
+            e.record()
+            torch.cuda.synchronize()
+            calls.append(a.elapsed_time(e))
+        e_ms = statistics.median(calls)
+        h2d = sum(hb["traces"].nbytes + 4 * hb["source_x"].nbytes for hb in host_bins) \
+            + host_v.numel() * 4
+        e2e = {"value": pairs / (e_ms * 1e-3) / 1e9, "unit": "Gpairs/s",
+               "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(2 * len(surveys) * int(np.prod(shape)) * 4),
+               "ms_per_step": e_ms, "ms_calls": [round(c, 1) for c in calls],
+               "api": "MigrationEngine.migrate_bins_full (plans, H2D, staging, batched launch, "
+                      "fold normalisation, D2H of every class image and fold)",
+               "outputs": out_kind}
+        del outs
+    n_tr = int(sum(sv.n_traces for sv in surveys))
+    res = {"metric": "PSTM Gpairs/s (out-sample x trace), batched classes",
+           "value": pairs / (ms * 1e-3) / 1e9, "unit": "Gpairs/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": args.storage, "data": "synthetic",
+           "config": {"workload": f"batched 3D PSTM: {len(surveys)} offset/azimuth classes, "
+                                  f"{n_tr} traces x {args.samples} samples, per-class "
                                   f"{args.grid}x{args.grid}x{args.samples} images, "
                                   f"{args.storage} storage, one persistent launch in a CUDA "
                                   "graph", "pairs_per_step": pairs, "datagen_s": t_gen,
+                      "class_shapes": {str(k): b.shapes.count(k) for k in sorted(set(b.shapes))},
+                      "class_shape_ids": b.shapes,
+                      "shape_choice": ("autotuner per class (cached per problem class), "
+                                       f"plans + choices {t_tune:.2f} s"
+                                       if args.variant == "auto" else "fixed --variant"),
+                      "launches_per_step": b.launches_per_replay,
                       "l2": "inputs larger than L2; no flush"},
-           "gpu_launches": int(b.launches_per_replay * args.steps),
-           "clocks": clk.summary()}
+           "roofline": roof, "error_vs_fp64": err, "cpu_baseline": cb, "e2e": e2e,
+           "gpu_launches": int(launches), "clocks": clk.summary()}
     print(json.dumps(res), flush=True)
     b.close()
-    for p in plans:
-        p.close()
+    for p_ in plans:
+        p_.close()
+
+
+def bench_batched_reference(args):
+    """Reference arm of the batched config: the reference algorithm (CPU port)
+    migrating the classes one bin at a time, as the reference worker does, on a
+    centred crop of each class with all its traces supplied."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import pstm_fp64 as O
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
+    surveys = batched_surveys(args, dev)
+    s0 = surveys[0]
+    cols = cpu_crop_columns(s0, args.crop)
+    il, xl = cols // s0.n_xl, cols % s0.n_xl
+    cx = s0.origin_x + il * s0.il_spacing
+    cy = s0.origin_y + xl * s0.xl_spacing
+    t_ms = (np.arange(s0.n_times, dtype=np.float32) * np.float32(s0.dt_ms)).astype(np.float64)
+    vmean = float(s0.vrms.mean())
+    pcs = [O.count_pairs_fp64(sv.source_x, sv.source_y, sv.receiver_x, sv.receiver_y, cx, cy,
+                              t_ms, vmean, sv.max_aperture_m, sv.max_angle_deg)
+           for sv in surveys]
+    vals, secs = [], []
+    for it in range(args.warmup + args.steps):
+        sec = sum(run_cpu_port(sv, cols, pc)["seconds"] for sv, pc in zip(surveys, pcs) if pc > 0)
+        if it >= args.warmup:
+            vals.append(sum(pcs) / sec / 1e9)
+            secs.append(sec)
+    v = statistics.median(vals)
+    cb = {"value": v, "unit": "Gpairs/s", "cores": len(os.sched_getaffinity(0)), "kind": "port",
+          "sample": f"every class with pairs in a centred {args.crop}x{args.crop}-column crop, "
+                    f"one bin at a time, {sum(pcs):.3e} pairs; constant V = mean V_rms"}
+    print(json.dumps({
+        "metric": "PSTM Gpairs/s (out-sample x trace), batched classes", "value": v,
+        "unit": "Gpairs/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": statistics.median(secs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": f"batched 3D PSTM: {len(surveys)} offset/azimuth classes, "
+                               f"{args.samples} samples, per-class {args.grid}x{args.grid} "
+                               "grids, the reference's one-bin-at-a-time loop on a crop"},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "Gpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
 
 
 def bench_lsq(args):
@@ -963,7 +1347,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
-    ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--variant", default="auto",
+                    help="kernel shape id, 0 for the library's heuristic, or auto (the tuner's "
+                         "choice per problem class)")
     ap.add_argument("--traces", type=int, default=500_000)
     ap.add_argument("--samples", type=int, default=1000)
     ap.add_argument("--grid", type=int, default=200)
@@ -971,24 +1357,31 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--err-crop", type=int, default=2,
-                    help="side of the column crop checked against the FP64 oracle")
+                    help="anti-alias workload: side of the centred crop the FP64 oracle is "
+                         "timed on as the CPU baseline")
+    ap.add_argument("--err-clusters", type=int, default=16,
+                    help="2x2 column clusters checked against the FP64 oracle (>= 9: corners, "
+                         "edge midpoints and centre come first)")
     ap.add_argument("--antialias", action="store_true",
                     help="triangle anti-alias filter (half-width from the operator dip)")
     ap.add_argument("--aa-lmax", type=float, default=32.0)
     ap.add_argument("--utm", action="store_true",
                     help="world coordinates offset by a UTM origin (5e5, 6e6) m")
+    ap.add_argument("--shard-mode", default="slabs", choices=["slabs", "replicas"],
+                    help="with N > 1 ranks: inline slabs of one survey (strong scaling) or one "
+                         "independent survey per rank (weak scaling)")
+    ap.add_argument("--classes", type=int, default=64,
+                    help="batched config: the first N of the 64 offset/azimuth classes")
     ap.add_argument("--lsq-traces", type=int, default=120_000)
     ap.add_argument("--cg-iters", type=int, default=10)
     ap.add_argument("--fd-directions", type=int, default=20)
     ap.add_argument("--config", default="3d",
                     choices=["3d", "batched", "lsq", "velocity", "time_rms"])
     args = ap.parse_args()
+    if args.variant != "auto":
+        args.variant = int(args.variant)
     if args.config == "batched":
-        if args.impl == "ours":
-            return bench_batched(args)
-        return bench_unavailable("the reference migrates offset/azimuth classes one bin at a "
-                                 "time through migrate_bin_full; its per-bin arm is the default "
-                                 "config")
+        return bench_batched(args) if args.impl == "ours" else bench_batched_reference(args)
     if args.config == "lsq":
         if args.impl == "ours":
             return bench_lsq(args)
@@ -1000,6 +1393,8 @@ def main():
         return bench_time_rms(args) if args.impl == "ours" else bench_time_rms_reference(args)
     if args.impl == "reference":
         bench_reference(args)
+    elif int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.shard_mode == "slabs":
+        bench_sharded(args)
     else:
         bench_ours(args)
 

@@ -100,7 +100,8 @@ typedef struct pstm_params {
   int32_t forward_only;        /* 1: the plan only migrates.  float32 rows are then staged in
                                   intercept form, one FMA per tap and ~3 % faster; the
                                   demigration stays its transpose to ~1e-5 (not float rounding)
-                                  and pstm_velocity_gradient / batches reject the plan.
+                                  and pstm_velocity_gradient rejects the plan; a batch takes
+                                  it when every class plan is forward_only.
                                   0: (x, dx) rows, migration and demigration an exact float
                                   transpose pair (dot-product tests, least squares). */
   double taper_width;          /* 0: hard masks only (what the reference migrators apply).

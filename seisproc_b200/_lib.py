@@ -11,7 +11,10 @@ import os
 import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libseispstm.so")
+# SEISPSTM_LIBRARY=checked loads the checked test build (bounds checks, short
+# device wait limit, fault injection) instead of the product library.
+CHECKED = os.environ.get("SEISPSTM_LIBRARY", "") == "checked"
+LIB_PATH = os.path.join(HERE, "libseispstm_checked.so" if CHECKED else "libseispstm.so")
 
 PSTM_OK, PSTM_EINVAL, PSTM_ENOMEM, PSTM_ETIMEOUT, PSTM_EBOUNDS, PSTM_ECUDA, PSTM_ENOTSUP = range(7)
 PSTM_F32, PSTM_BF16, PSTM_F16, PSTM_F64 = range(4)
@@ -118,12 +121,15 @@ def lib():
             return _lib
         if not os.path.exists(LIB_PATH):
             from . import build as _build
-            _build.build()
+            _build.build(checked=CHECKED)
         L = C.CDLL(LIB_PATH)
         for name, (res, args) in _SIGNATURES.items():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
+        if CHECKED:
+            L.pstm_test_set_injection.restype = C.c_int
+            L.pstm_test_set_injection.argtypes = [C.c_int32]
         _lib = L
         return _lib
 

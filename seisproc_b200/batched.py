@@ -21,7 +21,7 @@ from typing import Any, Dict, List, Optional, Sequence, Tuple
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, autotune
 from .kirchhoff import PSTMPlan, velocity_strides
 
 
@@ -130,10 +130,13 @@ def class_indices(offset: np.ndarray, azimuth: np.ndarray, n_offset_bins: int,
 
 
 class BatchedPSTM:
-    """All classes of a survey in one persistent launch.
+    """All classes of a survey in one persistent launch per kernel shape.
 
     ``plans`` share grid, parameters and storage; ``velocity`` is V_rms for all
-    classes.  Images (and folds) are allocated here, one per class.
+    classes.  Images (and folds) are allocated here, one per class.  Classes
+    whose plans have different kernel shapes (per-class tuning) are grouped by
+    shape, one persistent launch per group; ``shapes`` lists each class's
+    shape id and ``capture`` records every group's launch in the same graph.
     """
 
     def __init__(self, plans: Sequence[PSTMPlan], velocity: torch.Tensor, with_fold: bool = True):
@@ -148,25 +151,35 @@ class BatchedPSTM:
         self.images = [torch.zeros(shape, device=self.device) for _ in self.plans]
         self.folds = [torch.zeros(shape, device=self.device) for _ in self.plans] \
             if with_fold else None
-        n = len(self.plans)
-        P = C.c_void_p * n
-        plans_arr = P(*[p._handle.value for p in self.plans])
-        imgs = P(*[t.data_ptr() for t in self.images])
-        folds = P(*[t.data_ptr() for t in self.folds]) if with_fold else None
+        self.shapes = [int(p.stats()["variant"]) for p in self.plans]
         self._lib = _lib.lib()
-        self._handle = C.c_void_p(None)
-        _lib.check(self._lib.pstm_batch_create(C.byref(self._handle), plans_arr, n, imgs, folds,
-                                               self.velocity.data_ptr(), vst, vsc,
-                                               torch.cuda.current_stream().cuda_stream))
+        self._handles: List[C.c_void_p] = []
+        try:
+            for sid in sorted(set(self.shapes)):
+                idx = [i for i, v in enumerate(self.shapes) if v == sid]
+                P = C.c_void_p * len(idx)
+                plans_arr = P(*[self.plans[i]._handle.value for i in idx])
+                imgs = P(*[self.images[i].data_ptr() for i in idx])
+                folds = P(*[self.folds[i].data_ptr() for i in idx]) if with_fold else None
+                h = C.c_void_p(None)
+                _lib.check(self._lib.pstm_batch_create(
+                    C.byref(h), plans_arr, len(idx), imgs, folds, self.velocity.data_ptr(),
+                    vst, vsc, torch.cuda.current_stream().cuda_stream))
+                self._handles.append(h)
+        except Exception:
+            self.close()
+            raise
         self._graph: Optional[torch.cuda.CUDAGraph] = None
         self._inputs: List[torch.Tensor] = []
         self.launches_per_replay = 0
 
     def close(self):
-        if getattr(self, "_handle", None) is not None and self._handle.value:
+        if getattr(self, "_handles", None):
             self._graph = None
-            self._lib.pstm_batch_destroy(self._handle)
-            self._handle = C.c_void_p(None)
+            for h in self._handles:
+                if h.value:
+                    self._lib.pstm_batch_destroy(h)
+            self._handles = []
         if getattr(self, "_own_plans", False):
             for p in self.plans:
                 p.close()
@@ -183,8 +196,8 @@ class BatchedPSTM:
             p.load_traces(t)
 
     def migrate(self) -> None:
-        _lib.check(self._lib.pstm_batch_migrate(self._handle,
-                                                torch.cuda.current_stream().cuda_stream))
+        for h in self._handles:
+            _lib.check(self._lib.pstm_batch_migrate(h, torch.cuda.current_stream().cuda_stream))
 
     def check(self) -> None:
         for p in self.plans:
@@ -200,7 +213,9 @@ class BatchedPSTM:
         class (``plan_kwargs`` as for ``PSTMPlan``: grid, axes, aperture ...).
         ``traces`` (n_samples, n_traces) stay on the device; each class's traces
         are gathered into ``self.class_traces`` and loaded.  ``self.bins`` and
-        ``self.indices`` name the classes and their traces."""
+        ``self.indices`` name the classes and their traces.  ``variant="auto"``
+        picks each class's kernel shape with the autotuner (cached per problem
+        class)."""
         dev = traces.device
         idx = bin_indices(source_x.to(dev), source_y.to(dev), receiver_x.to(dev),
                           receiver_y.to(dev), bins)
@@ -211,7 +226,12 @@ class BatchedPSTM:
         for _, i in keep:
             coords = [a.to(dev).index_select(0, i).contiguous()
                       for a in (source_x, source_y, receiver_x, receiver_y)]
-            plans.append(PSTMPlan(*coords, **plan_kwargs))
+            kw = dict(plan_kwargs)
+            if kw.get("variant") == "auto":
+                kw["variant"] = autotune.choose_variant(coords, velocity=velocity.to(dev),
+                                                        **{k: v for k, v in kw.items()
+                                                           if k != "variant"})
+            plans.append(PSTMPlan(*coords, **kw))
             class_traces.append(traces.index_select(1, i).contiguous())
         batch = cls(plans, velocity, with_fold=with_fold)
         batch._own_plans = True

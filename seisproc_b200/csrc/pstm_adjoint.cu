@@ -307,7 +307,10 @@ cudaError_t adj_dispatch(const Plan* p, const KArgs& A, const float4* tab, cudaS
       return adj_wm<2, 4, 2>(p, A, tab, s);
     case 3:
     case 9:
-      // 4 samples per lane (128-sample windows) at 40 registers, three CTAs
+    case 10:
+    case 11:
+    case 12:
+      // 16-column tiles, whatever the forward window: 4 samples per lane (128-sample windows) at 40 registers, three CTAs
       // (48 warps) per SM to hide the latency of the shared-memory adds:
       // 1.65x faster than 16 samples per lane at 128 registers and one CTA
       // per SM (two CTAs at 8 samples per lane: 1.6x)

@@ -60,7 +60,7 @@ template <int COLS, int WPC, int M, typename ST>
 cudaError_t batch_wm(const Batch* b, cudaStream_t s) {
   const Plan* p = b->plans[0];
   const bool lc = needs_lowclamp(p);
-  if constexpr (!std::is_same<ST, float2>::value) {
+  if constexpr (!std::is_same<ST, float2>::value && !std::is_same<ST, RowIcpt>::value) {
     if (p->params.weight != W_OBL_SPREAD) return cudaErrorNotSupported;
     return lc ? launch_batch_one<COLS, WPC, M, ST, W_OBL_SPREAD, true>(b, s)
               : launch_batch_one<COLS, WPC, M, ST, W_OBL_SPREAD, false>(b, s);
@@ -87,7 +87,9 @@ template <int COLS, int WPC, int M>
 cudaError_t batch_st(const Batch* b, cudaStream_t s) {
   switch (b->plans[0]->params.storage) {
     case PSTM_F32:
-      return batch_wm<COLS, WPC, M, float2>(b, s);
+      // forward_only class plans stage intercept-form rows, the others (x, dx)
+      return b->plans[0]->row_origin != 0 ? batch_wm<COLS, WPC, M, RowIcpt>(b, s)
+                                          : batch_wm<COLS, WPC, M, float2>(b, s);
     case PSTM_BF16:
       return batch_wm<COLS, WPC, M, __nv_bfloat16>(b, s);
     case PSTM_F16:
@@ -112,6 +114,11 @@ cudaError_t batch_dispatch(const Batch* b, cudaStream_t s) {
     case 3:
     case 9:
       return batch_st<16, 1, 8>(b, s);
+    case 10:
+    case 12:
+      return batch_st<16, 1, 4>(b, s);
+    case 11:
+      return batch_st<16, 1, 2>(b, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -153,11 +160,6 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
       return bfail(PSTM_ENOTSUP, "the batched launch applies no aperture taper or curved rays: "
                                  "build the class plans without taper_width or ray_gradient");
     }
-    if (p->params.forward_only && p->params.storage == PSTM_F32) {
-      free_batch(b);
-      return bfail(PSTM_ENOTSUP, "the batched launch reads (x, dx) float32 rows: build the "
-                                 "class plans without forward_only");
-    }
     // the descriptors capture the staging buffers, so they must exist now
     const pstm_status st = ensure_trace_storage(p, s);
     if (st != PSTM_OK) {
@@ -172,10 +174,10 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
     if (p->shape.id != p0->shape.id || p->params.storage != p0->params.storage ||
         p->params.weight != p0->params.weight || p->row_stride != p0->row_stride ||
         p->grid.n_times != p0->grid.n_times || p->params.clamp != p0->params.clamp ||
-        needs_lowclamp(p) != needs_lowclamp(p0)) {
+        needs_lowclamp(p) != needs_lowclamp(p0) || p->row_origin != p0->row_origin) {
       free_batch(b);
       return bfail(PSTM_EINVAL, "batched plans must share kernel shape, storage, weight, clamp, "
-                                "time axis and trace length");
+                                "time axis, trace length and forward_only");
     }
     b->plans.push_back(p);
     b->images.push_back(images[i]);

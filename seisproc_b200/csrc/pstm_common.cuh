@@ -12,8 +12,11 @@
 #define PSTM_ERR_COORDS 8
 
 // Bounded waits on an mbarrier give up after this many nanoseconds of the
-// global timer (2 s: far beyond any legitimate wait for one pipeline stage).
+// global timer (2 s: far beyond any legitimate wait for one pipeline stage;
+// the checked test build shortens it).
+#ifndef PSTM_WAIT_NS
 #define PSTM_WAIT_NS 2000000000ull
+#endif
 
 namespace pstm {
 

@@ -21,6 +21,8 @@ struct TaperArgs {
   float a0, ainv, amax, tan2;
 };
 
+constexpr uint32_t kMagicBitsC = 0x4B000000u;  // float bits of 2^23
+
 struct KArgs {
   const float4* geo;
   const int* list;
@@ -52,7 +54,50 @@ struct KArgs {
   // curved rays (plans built with a ray gradient k): k, and 1000 / (k in_dt)
   // turning the summed arccosh of the two legs into an input sample index
   float cr_k, cr_scale;
+  long long n_traces;  // rows staged (bounds of the list entries)
+  int inject;          // checked test build only: the fault to simulate (0 = none)
 };
+
+// Faults the checked test build can simulate (pstm_test_set_injection); the
+// product build never reads KArgs::inject.
+enum Inject { INJ_NONE = 0, INJ_MISSING_COPY = 1, INJ_NO_CLAMP = 2, INJ_BAD_LIST_ENTRY = 3 };
+
+// Trace-list entry at position pos.  The checked build (PSTM_BOUNDS_CHECK)
+// verifies it before any use -- an entry outside [0, n_traces) raises
+// PSTM_ERR_BOUNDS and is replaced by 0 -- and can simulate a corrupted first
+// entry of the lists to exercise that path.
+__device__ __forceinline__ int list_entry(const KArgs& A, int64_t pos) {
+  int jj = A.list[pos];
+#ifdef PSTM_BOUNDS_CHECK
+  if (A.inject == INJ_BAD_LIST_ENTRY && pos == 0)
+    jj = (int)(A.n_traces + 1000 < 0x7fffffffLL ? A.n_traces + 1000 : 0x7fffffffLL);
+  if (jj < 0 || (long long)jj >= A.n_traces) {
+    set_error(A.err, PSTM_ERR_BOUNDS);
+    jj = 0;
+  }
+#endif
+  return jj;
+}
+
+// Checked build: the entry index a staged-row read addresses (from the float
+// bits of the floored index) must lie in [lo, hi] of the row as staged;
+// otherwise PSTM_ERR_BOUNDS is raised and the read goes to entry 0 instead.
+// The product build compiles this to nothing.
+struct RowCheck {
+  int lo, hi;
+  int* err;
+};
+__device__ __forceinline__ uint32_t checked_addr(uint32_t addr, uint32_t bits, uint32_t base,
+                                                 int shift, const RowCheck& rc) {
+#ifdef PSTM_BOUNDS_CHECK
+  const int e = (int)(bits - kMagicBitsC);
+  if (e < rc.lo || e > rc.hi) {
+    set_error(rc.err, PSTM_ERR_BOUNDS);
+    return base + (kMagicBitsC << shift);
+  }
+#endif
+  return addr;
+}
 
 __device__ __forceinline__ float vel_at(const KArgs& A, int k, int c) {
   return __ldg(A.vel + (long long)k * A.vst + (long long)c * A.vsc);
@@ -204,6 +249,8 @@ inline KArgs make_args(const Plan* p, const float* vel, int64_t vst, int64_t vsc
     A.tp.amax = (float)th;
     A.tp.tan2 = (float)(std::tan(a0) * std::tan(a0));
   }
+  A.n_traces = p->n_traces;
+  A.inject = test_injection();
   A.cr_k = (float)p->params.ray_gradient;
   A.cr_scale = p->params.ray_gradient != 0
                    ? (float)(1000.0 / (p->params.ray_gradient * p->params.in_dt_ms))

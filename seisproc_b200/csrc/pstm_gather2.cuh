@@ -107,7 +107,8 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
                                              const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
                                              const float (&sc)[NTR], f2 bb, f2 magic2,
                                              float hi_c, float lo_c, int kw, int lane, int g0,
-                                             const TaperArgs& tp, float cr_scale = 0.f) {
+                                             const TaperArgs& tp, float cr_scale = 0.f,
+                                             RowCheck rc = RowCheck{}) {
   // curved rays: zz = z^2 + f, aa = k / (2 v0 max(z, 1e-6)); no pre-scaling
   constexpr bool PRE = kPrescaled<OP, WM> && !CURVED;
   constexpr int ES = (int)sizeof(ST);
@@ -156,8 +157,10 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
         id.y = fmaxf(id.y, lo_c);
       }
       const f2 tm = f2_add_rm(id, magic2);
-      const uint32_t a0 = rbase[n] + (__float_as_uint(tm.x) << SHIFT);
-      const uint32_t a1 = rbase[n] + (__float_as_uint(tm.y) << SHIFT);
+      const uint32_t a0 = checked_addr(rbase[n] + (__float_as_uint(tm.x) << SHIFT),
+                                       __float_as_uint(tm.x), rbase[n], SHIFT, rc);
+      const uint32_t a1 = checked_addr(rbase[n] + (__float_as_uint(tm.y) << SHIFT),
+                                       __float_as_uint(tm.y), rbase[n], SHIFT, rc);
       f2 dx, amp;
       if constexpr (std::is_same<ST, float2>::value) {
         // expanded rows: one 8-byte load gives (x[i0], x[i0+1] - x[i0])
@@ -238,6 +241,42 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
   }
 }
 
+// A masked sweep (some trace starts inside the warp's segment) entered at g0,
+// the first group holding a contributing sample, through a jump table: the
+// groups from g0 on run as one straight-line block, each group masked by
+// sample index, with no per-group branch (measured 1.3 % faster than testing
+// every group against g0).
+#define PSTM_SWEEP_GROUP(I)                                                                     \
+  if constexpr ((I) < M) {                                                                      \
+    sweep_traces<1, ST, WM, LOWC, true, OP, NTR, TAPER, CURVED>(                                \
+        reinterpret_cast<f2(&)[1]>(acc[(I) % M]), reinterpret_cast<const f2(&)[1]>(zz[(I) % M]), \
+        reinterpret_cast<const f2(&)[1]>(aa[(I) % M]), hs2, hr2, rbase, kst, sc, bb, magic2,     \
+        hi_c, lo_c, kw + 64 * (I), lane, 0, tp, cr_scale, rc);                                  \
+  }
+template <int M, typename ST, int WM, bool LOWC, int OP, int NTR, bool TAPER, bool CURVED>
+__device__ __forceinline__ void sweep_masked_from(f2 (&acc)[M], const f2 (&zz)[M],
+                                                  const f2 (&aa)[M], const float (&hs2)[NTR],
+                                                  const float (&hr2)[NTR],
+                                                  const uint32_t (&rbase)[NTR],
+                                                  const int (&kst)[NTR], const float (&sc)[NTR],
+                                                  f2 bb, f2 magic2, float hi_c, float lo_c, int kw,
+                                                  int lane, int g0, const TaperArgs& tp,
+                                                  float cr_scale, RowCheck rc) {
+  static_assert(M <= 8, "the jump table covers up to 8 groups");
+  switch (g0 < 0 ? 0 : g0) {
+    case 0: PSTM_SWEEP_GROUP(0) [[fallthrough]];
+    case 1: PSTM_SWEEP_GROUP(1) [[fallthrough]];
+    case 2: PSTM_SWEEP_GROUP(2) [[fallthrough]];
+    case 3: PSTM_SWEEP_GROUP(3) [[fallthrough]];
+    case 4: PSTM_SWEEP_GROUP(4) [[fallthrough]];
+    case 5: PSTM_SWEEP_GROUP(5) [[fallthrough]];
+    case 6: PSTM_SWEEP_GROUP(6) [[fallthrough]];
+    case 7: PSTM_SWEEP_GROUP(7) [[fallthrough]];
+    default: break;
+  }
+}
+#undef PSTM_SWEEP_GROUP
+
 // One output tile x time window: the body shared by the per-plan grid kernel
 // (one CTA per tile/window) and the persistent batched kernel (one work item
 // at a time).  Barriers are (re)initialised on entry; every bulk copy issued
@@ -255,12 +294,14 @@ __device__ __forceinline__ void sweep_aa(f2 (&acc)[M], const f2 (&zz)[M], const 
                                          const float (&gys)[NTR], const float (&gyr)[NTR],
                                          const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
                                          f2 bb, f2 magic2, float hi_c, float lo_c, float lmax,
-                                         int kw, int lane, int g0) {
+                                         int kw, int lane, int g0, RowCheck rc = RowCheck{}) {
   auto tap = [&](f2 pos, uint32_t base) {
     // expanded rows: intercept and slope of I2's piece, one FMA of the position
     const f2 tm = f2_add_rm(pos, magic2);
-    const f2 e0 = lds_f2(base + (__float_as_uint(tm.x) << 3));
-    const f2 e1 = lds_f2(base + (__float_as_uint(tm.y) << 3));
+    const f2 e0 = lds_f2(checked_addr(base + (__float_as_uint(tm.x) << 3),
+                                      __float_as_uint(tm.x), base, 3, rc));
+    const f2 e1 = lds_f2(checked_addr(base + (__float_as_uint(tm.y) << 3),
+                                      __float_as_uint(tm.y), base, 3, rc));
     return f2{fmaf(pos.x, e0.y, e0.x), fmaf(pos.y, e1.y, e1.x)};
   };
 #pragma unroll
@@ -369,8 +410,13 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     const int cnt = min(B, n_list - b * B);
     if (lane == 0) mbar_arrive_expect_tx(full + s, bytes * cnt);
     __syncwarp();
+#ifdef PSTM_BOUNDS_CHECK
+    // simulated fault: block 1 of the first item is never copied, so the
+    // consumers' bounded waits on its stage expire
+    if (A.inject == INJ_MISSING_COPY && tile == 0 && win == 0 && b == 1) return;
+#endif
     if (lane < cnt) {
-      const int jj = A.list[off0 + (int64_t)b * B + lane];
+      const int jj = list_entry(A, off0 + (int64_t)b * B + lane);
       bulk_g2s(raw + (s * B + lane) * RP + kRowGuard,
                reinterpret_cast<const ST*>(A.traces) + (int64_t)jj * S + lo, bytes, full + s);
     }
@@ -426,8 +472,16 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   const f2 mg = f2_bcast(AA || kIcpt ? kMagic + (float)(A.row_origin - lo) : kMagic);
   const float bconst = -A.in_t0 / A.in_dt + shift;
   const f2 bb = f2_bcast(bconst);
+#ifdef PSTM_BOUNDS_CHECK
+  // simulated fault: no upper clamp, so late samples index past the staged row
+  const float hi_c = A.inject == INJ_NO_CLAMP ? 1.0e30f : A.clamp_hi + shift;
+#else
   const float hi_c = A.clamp_hi + shift;
+#endif
   const float lo_c = shift;  // idx >= 0 (LOWC: output times before the first input)
+  // entries a staged-row read may address: the guard before the row, then
+  // the rowlen entries copied (16-bit and plain float32 rows read two)
+  const RowCheck rck{-kRowGuard / ES, rowlen - (ES == 8 ? 1 : 2), A.err};
   const float* thr_c = thr + cl * T;
   const uint32_t raw_base = smem_addr(raw) + kRowGuard - (kMagicBits << SHIFT);
   const int kwe = kw + 64 * M;
@@ -437,7 +491,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   uint32_t phase = 0;
   // the next chunk's list entries and geometry are fetched while the current
   // chunk computes
-  int jj_next = (lane < n_list) ? A.list[off0 + lane] : 0;
+  int jj_next = (lane < n_list) ? list_entry(A, off0 + lane) : 0;
   float4 g_next = make_float4(0.f, 0.f, 0.f, 0.f);
   if (warp_live && lane < n_list) g_next = __ldg(A.geo + jj_next);
   for (int p0 = 0; p0 < n_list && !aborted; p0 += 32) {
@@ -472,7 +526,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
       }
     }
     const int pn = p0 + 32 + lane;
-    if (pn < n_list) jj_next = A.list[off0 + pn];
+    if (pn < n_list) jj_next = list_entry(A, off0 + pn);
     const int nt = min(32, n_list - p0);
     for (int t = 0; t < nt;) {
       const int p = p0 + t;
@@ -512,10 +566,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
           const int kk[1] = {kq};
           if (kq > kw)
             sweep_aa<M, LOWC, true, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, mg, hi_c,
-                                       lo_c, A.aa_lmax, kw, lane, (kq - kw) >> 6);
+                                       lo_c, A.aa_lmax, kw, lane, (kq - kw) >> 6, rck);
           else
             sweep_aa<M, LOWC, false, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, mg, hi_c,
-                                        lo_c, A.aa_lmax, kw, lane, 0);
+                                        lo_c, A.aa_lmax, kw, lane, 0, rck);
         }
       } else if (la && lb) {
         const float hs[2] = {__shfl_sync(0xffffffffu, hs2, t), __shfl_sync(0xffffffffu, hs2, t + 1)};
@@ -524,14 +578,13 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const uint32_t rb[2] = {rb0, rb0 + (uint32_t)RP};
         const int kk[2] = {ka, kb};
         if (ka > kw || kb > kw)
-          sweep_traces<M, ST, WM, LOWC, true, OP, 2, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
-                                                             hi_c, lo_c, kw, lane,
-                                                             (min(ka, kb) - kw) >> 6, A.tp,
-                                                             A.cr_scale);
+          sweep_masked_from<M, ST, WM, LOWC, OP, 2, TAPER, CURVED>(
+              acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c, lo_c, kw, lane,
+              (min(ka, kb) - kw) >> 6, A.tp, A.cr_scale, rck);
         else
           sweep_traces<M, ST, WM, LOWC, false, OP, 2, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
                                                               hi_c, lo_c, kw, lane, 0, A.tp,
-                                                              A.cr_scale);
+                                                              A.cr_scale, rck);
       } else if (la || lb) {
         const int u = la ? t : t + 1;
         const float hs[1] = {__shfl_sync(0xffffffffu, hs2, u)};
@@ -540,13 +593,13 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const uint32_t rb[1] = {la ? rb0 : rb0 + (uint32_t)RP};
         const int kk[1] = {la ? ka : kb};
         if (kk[0] > kw)
-          sweep_traces<M, ST, WM, LOWC, true, OP, 1, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
-                                                             hi_c, lo_c, kw, lane, (kk[0] - kw) >> 6,
-                                                             A.tp, A.cr_scale);
+          sweep_masked_from<M, ST, WM, LOWC, OP, 1, TAPER, CURVED>(
+              acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c, lo_c, kw, lane, (kk[0] - kw) >> 6,
+              A.tp, A.cr_scale, rck);
         else
           sweep_traces<M, ST, WM, LOWC, false, OP, 1, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
                                                               hi_c, lo_c, kw, lane, 0, A.tp,
-                                                              A.cr_scale);
+                                                              A.cr_scale, rck);
       }
       const int adv = pair ? 2 : 1;
       t += adv;
@@ -782,6 +835,11 @@ inline cudaError_t dispatch2_shape(const Plan* p, const KArgs& A, cudaStream_t s
     case 3:
     case 9:
       return dispatch2_st<16, 1, 8, OP>(p, A, s);
+    case 10:
+    case 12:
+      return dispatch2_st<16, 1, 4, OP>(p, A, s);
+    case 11:
+      return dispatch2_st<16, 1, 2, OP>(p, A, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -21,6 +21,11 @@ cudaError_t launch_forward_icpt(const Plan* p, const KArgs& A, cudaStream_t s) {
     case 3:
     case 9:
       return dispatch2_wm<16, 1, 8, RowIcpt, OP_FWD>(p, A, s);
+    case 10:
+    case 12:
+      return dispatch2_wm<16, 1, 4, RowIcpt, OP_FWD>(p, A, s);
+    case 11:
+      return dispatch2_wm<16, 1, 2, RowIcpt, OP_FWD>(p, A, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -75,6 +75,9 @@ pstm_status launch_vgrad(Plan* p, const float* grad_image, const float* vel, int
 pstm_status launch_velocity_check(Plan* p, const float* vel, int64_t vst, int64_t vsc,
                                   cudaStream_t s, std::string* why);
 bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out);
+// Fault simulated by the checked test build's kernels (set by its
+// pstm_test_set_injection); always 0 in the product build.
+int test_injection();
 size_t forward_smem_bytes(const Plan* p);
 void count_launch();
 // Device memory of plans and their temporaries: stream-ordered allocations from

@@ -42,6 +42,9 @@ static std::atomic<int64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 int64_t launch_total() { return g_launches.load(); }
 
+static std::atomic<int> g_inject{0};
+int test_injection() { return g_inject.load(std::memory_order_relaxed); }
+
 // ---------------------------------------------------------------------------
 // Fold: number of traces inside the masks per output sample.  Counts the same
 // k_start values as the gather kernel (same threshold table and search).
@@ -76,7 +79,7 @@ __global__ void __launch_bounds__(256) pstm_fold_kernel(const KArgs A) {
     if (ok[q]) column_xy(A, qil, qxl, qx[q], qy[q]);
   }
   for (int t = threadIdx.x; t < n_list; t += blockDim.x) {
-    const float4 g = __ldg(A.geo + A.list[off0 + t]);
+    const float4 g = __ldg(A.geo + list_entry(A, off0 + t));
 #pragma unroll
     for (int q = 0; q < COLS; ++q) {
       if (!ok[q]) continue;
@@ -142,6 +145,9 @@ static const Shape kShapes[] = {
     {7, 2, 4, 2, 2, 1},  // 2D lines: 2 inlines x 512 samples
     {8, 4, 4, 4, 4, 1},  // 2D lines: 4 inlines x 1024 samples
     {9, 16, 1, 8, 16, 1},  // 2D lines: 16 inlines x 512 samples
+    {10, 16, 1, 4, 4, 4},  // 16 columns (4x4) x 256 samples
+    {11, 16, 1, 2, 4, 4},  // 16 columns (4x4) x 128 samples
+    {12, 16, 1, 4, 16, 1},  // 2D lines: 16 inlines x 256 samples
 };
 
 bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out) {
@@ -220,3 +226,18 @@ pstm_status launch_fold(Plan* p, const float* vel, int64_t vst, int64_t vsc, flo
 }
 
 }  // namespace pstm
+
+#ifdef PSTM_CHECKED_BUILD
+// The checked test build (libseispstm_checked.so: bounds checks on, 50 ms wait
+// limit) exports one more entry point: the fault its kernels simulate on the
+// next launches, so the tests can drive the failure paths without faulting a
+// GPU -- a stage copy that is never issued (the bounded waits expire:
+// PSTM_ETIMEOUT), the upper index clamp left out (staged-row reads beyond the
+// row, caught by the bounds checks: PSTM_EBOUNDS), a trace-list entry out of
+// range (caught before it is used: PSTM_EBOUNDS).  0 restores normal runs.
+extern "C" pstm_status pstm_test_set_injection(int32_t kind) {
+  if (kind < pstm::INJ_NONE || kind > pstm::INJ_BAD_LIST_ENTRY) return PSTM_EINVAL;
+  pstm::g_inject.store(kind);
+  return PSTM_OK;
+}
+#endif

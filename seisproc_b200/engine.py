@@ -29,6 +29,7 @@ from typing import Callable, Optional, Tuple
 import numpy as np
 import torch
 
+from . import autotune
 from .kernel_backend import require_cuda
 from .kirchhoff import PSTMPlan, normalize_by_fold
 from . import models as _models
@@ -63,7 +64,10 @@ class MigrationEngine:
     CPU; this engine only runs on CUDA and raises otherwise)."""
 
     def __init__(self, device: Optional[torch.device] = None, kernel_backend=None,
-                 storage: str = "f32", variant: int = 0):
+                 storage: str = "f32", variant="auto"):
+        """``variant``: the kernel shape id, 0 for the library's heuristic, or
+        "auto" (default) for the autotuner's choice per problem class (cached;
+        a miss costs one timing run on a crop of the grid)."""
         require_cuda(kernel_backend)
         if device is None:
             device = torch.device("cuda", torch.cuda.current_device())
@@ -213,6 +217,140 @@ class MigrationEngine:
                              use_time_dependent_aperture, velocity_model, kernel_backend,
                              antialias, aa_max_halfwidth)
 
+    def migrate_bins_full(
+        self,
+        bins,
+        origin_x: float,
+        origin_y: float,
+        il_spacing: float,
+        xl_spacing: float,
+        azimuth_deg: float,
+        n_il: int,
+        n_xl: int,
+        dt_ms: float,
+        t_min_ms: float,
+        n_times: int = None,
+        velocity_mps: float = 2500.0,
+        max_aperture_m: float = 5000.0,
+        max_angle_deg: float = 60.0,
+        normalize: bool = True,
+        min_fold: int = 1,
+        progress_callback: Optional[Callable[[float, str], None]] = None,
+        use_time_dependent_aperture: bool = False,
+        velocity_model=None,
+        kernel_backend=None,
+        out=None,
+    ):
+        """``migrate_bin_full`` for many bins (offset/azimuth classes) at once.
+
+        The reference's worker migrates the classes of a survey one bin after
+        another (views/migration_monitor_dialog.py:201-430); here every bin
+        gets its own plan and all of them run in one persistent launch of the
+        batched kernel (``BatchedPSTM``), each into its own image (common-image
+        gathers).  ``bins`` is a sequence of mappings with ``traces``
+        ((n_samples, n_traces) float32), ``source_x``, ``source_y``,
+        ``receiver_x`` and ``receiver_y``; the grid, time axis, velocity and
+        aperture arguments are shared and mean what they mean for
+        ``migrate_bin_full``.  Returns one (image, fold) pair per bin, each
+        (n_times, n_il, n_xl) float32: new numpy arrays, or the buffers of
+        ``out`` (a sequence of (image, fold) host arrays or CPU tensors; page-
+        locked tensors receive the copies at full bus speed)."""
+        from . import _lib
+        from .batched import BatchedPSTM
+        require_cuda(kernel_backend if kernel_backend is not None else self.kernel_backend)
+        bins = list(bins)
+        if not bins:
+            raise ValueError("no bins to migrate")
+        if out is not None and len(out) != len(bins):
+            raise ValueError("out must hold one (image, fold) pair per bin")
+        n_s = int(np.asarray(bins[0]["traces"]).shape[0])
+        n_t = int(n_times) if n_times is not None else n_s
+        if progress_callback:
+            progress_callback(0.0, "Preparing data...")
+        L = _lib.lib()
+        with torch.cuda.device(self.device):
+            cur = torch.cuda.current_stream(self.device)
+            t_ms = np.arange(n_t, dtype=np.float32) * np.float32(dt_ms) + np.float32(t_min_ms)
+            il = np.arange(n_il)[:, None]
+            xl = np.arange(n_xl)[None, :]
+            col_x = (origin_x + il * il_spacing + 0 * xl).ravel()
+            col_y = (origin_y + 0 * il + xl * xl_spacing).ravel()
+            vel_t = self._velocity_grid(velocity_mps, velocity_model, t_ms, col_x, col_y)
+            kw = dict(n_il=n_il, n_xl=n_xl, n_times=n_t, origin_x=origin_x, origin_y=origin_y,
+                      il_dx=il_spacing, il_dy=0.0, xl_dx=0.0, xl_dy=xl_spacing, t0_ms=t_min_ms,
+                      dt_ms=dt_ms, n_samples=n_s, in_t0_ms=t_min_ms, in_dt_ms=dt_ms,
+                      max_aperture_m=max_aperture_m, max_angle_deg=max_angle_deg,
+                      time_dependent_aperture=use_time_dependent_aperture,
+                      storage=self.storage, variant=self.variant,
+                      kernel_backend=kernel_backend or self.kernel_backend, forward_only=True)
+            plans, batch = [], None
+            try:
+                for b in bins:
+                    tr = np.asarray(b["traces"])
+                    if tr.ndim != 2 or tr.shape[0] != n_s:
+                        raise ValueError("every bin's traces must be (n_samples, n_traces) with "
+                                         f"n_samples = {n_s}")
+                    coords = []
+                    for key in ("source_x", "source_y", "receiver_x", "receiver_y"):
+                        a = np.asarray(b[key])
+                        a = a.astype(np.float64 if a.dtype == np.float64 else np.float32)
+                        coords.append(torch.from_numpy(np.ascontiguousarray(a)).to(self.device))
+                    bkw = dict(kw)
+                    if bkw["variant"] == "auto":
+                        bkw["variant"] = autotune.choose_variant(
+                            coords, velocity=vel_t,
+                            **{k: v for k, v in bkw.items() if k != "variant"})
+                    plan = PSTMPlan(*coords, **bkw)
+                    plans.append(plan)
+                    host = np.ascontiguousarray(tr, dtype=np.float32)
+                    dev_tr = torch.empty((n_s, host.shape[1]), dtype=torch.float32,
+                                         device=self.device)
+                    if host.shape[1] > 0:
+                        _lib.check(L.pstm_copy_trace_columns(
+                            dev_tr.data_ptr(), host.ctypes.data, n_s, host.shape[1], 0,
+                            host.shape[1], cur.cuda_stream))
+                    plan.load_traces(dev_tr)
+                if progress_callback:
+                    progress_callback(0.1, "Running Kirchhoff migration...")
+                batch = BatchedPSTM(plans, vel_t)
+                batch.migrate()
+                batch.check()
+                if progress_callback:
+                    progress_callback(0.9, "Normalizing...")
+                results = []
+                for i, (img, fold) in enumerate(zip(batch.images, batch.folds)):
+                    if normalize:
+                        img = normalize_by_fold(img, fold, min_fold)
+                    if out is not None:
+                        for dst, src in zip(out[i], (img, fold)):
+                            if isinstance(dst, torch.Tensor):
+                                dst.copy_(src.reshape(dst.shape), non_blocking=dst.is_pinned())
+                            else:
+                                np.copyto(dst, src.reshape(dst.shape).cpu().numpy())
+                        results.append(tuple(out[i]))
+                    else:
+                        results.append(self._download(img, fold))
+                cur.synchronize()
+            finally:
+                if batch is not None:
+                    batch.close()
+                for plan in plans:
+                    plan.close()
+        if progress_callback:
+            progress_callback(1.0, "Complete")
+        return results
+
+    def _velocity_grid(self, velocity_mps, velocity_model, t_ms, col_x, col_y) -> torch.Tensor:
+        """V_rms at the output samples on the device (constant, V(t0) or V(t0, column))."""
+        if isinstance(velocity_model, _models.VelocityModel) and \
+                velocity_model.velocity_type in (_models.VelocityType.V_OF_XZ,
+                                                 _models.VelocityType.V_OF_XYZ):
+            return velocity_grid(velocity_model, np.asarray(t_ms, np.float64) / 1000.0, col_x,
+                                 col_y, self.device)
+        vel = np.ascontiguousarray(velocity_at_outputs(velocity_mps, velocity_model, t_ms, col_x,
+                                                       col_y))
+        return torch.from_numpy(vel).to(self.device)
+
     def _migrate(self, upload, n_s, n_tr, source_x, source_y, receiver_x, receiver_y, origin_x,
                  origin_y, il_spacing, xl_spacing, n_il, n_xl, dt_ms, t_min_ms, n_times,
                  velocity_mps, max_aperture_m, max_angle_deg, normalize, min_fold,
@@ -282,6 +420,10 @@ class MigrationEngine:
                       kernel_backend=kernel_backend or self.kernel_backend,
                       antialias=antialias, aa_dx=il_spacing, aa_dy=xl_spacing,
                       aa_max_halfwidth=aa_max_halfwidth, forward_only=True)
+            if kw["variant"] == "auto":
+                kw["variant"] = autotune.choose_variant(coords, velocity=vel_t,
+                                                        **{k: v for k, v in kw.items()
+                                                           if k != "variant"})
             plans = []
             try:
                 # every plan is built before the first launch (the builds
@@ -309,6 +451,7 @@ class MigrationEngine:
                 self.last_stats = {k: sum(p.stats()[k] for p in plans)
                                    for k in ("n_traces", "list_entries", "device_bytes")}
                 self.last_stats["blocks"] = len(plans)
+                self.last_stats["variant"] = plans[0].stats()["variant"]
                 self.last_stats["kernel_ms"] = ev0.elapsed_time(ev1)
                 if enable_profiling:
                     pairs = float(fold.double().sum().item())

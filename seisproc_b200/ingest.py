@@ -11,9 +11,11 @@ the plan stages them from that layout directly, so the host transpose and the
 pageable copy disappear and reading overlaps the upload.
 
 ``NumpyDataReader`` keeps the reference's interface; ``SegyDataReader`` reads a
-SEG-Y file through a memory map (IEEE or IBM float samples).  zarr is not
-installed here, so there is no ``ZarrDataReader``: any object with
-``read_traces`` and ``get_n_samples`` can be streamed.
+SEG-Y file through a memory map (IEEE or IBM float samples); ``ZarrDataReader``
+reads an uncompressed zarr format-2 trace array (the layout the reference's
+import and ``MigrationOutputStorage`` write) without the zarr package, which is
+not installed here.  Any object with ``read_traces`` and ``get_n_samples`` can
+be streamed.
 """
 from __future__ import annotations
 
@@ -94,6 +96,55 @@ class SegyDataReader(DataReader):
     @property
     def n_traces(self) -> int:
         return self._map.shape[0]
+
+
+class ZarrDataReader(DataReader):
+    """Traces from a zarr format-2 array, as the reference's reader takes them
+    (seisio/gather_readers.py:145-262): ``zarr_path`` is the array or a
+    directory holding ``traces.zarr``; the array is (n_samples, n_traces)
+    ("transposed", the reference's import layout) when ``metadata.json`` beside
+    it gives n_samples and n_traces matching its shape, else (n_traces,
+    n_samples).  Uncompressed float32 arrays only (no zarr package here):
+    compressed arrays raise ``ValueError``."""
+
+    def __init__(self, zarr_path: Union[str, Path]):
+        import json
+        from .output_storage import ZarrV2Array
+        zarr_path = Path(zarr_path)
+        if zarr_path.name == "traces.zarr" or (zarr_path / ".zarray").exists():
+            array_path, meta_path = zarr_path, zarr_path.parent / "metadata.json"
+        elif (zarr_path / "traces.zarr").exists():
+            array_path, meta_path = zarr_path / "traces.zarr", zarr_path / "metadata.json"
+        else:
+            raise ValueError(f"No valid Zarr array found at {zarr_path}")
+        self._z = ZarrV2Array.open(array_path)
+        self._transposed = False
+        self._n_traces, self._n_samples = self._z.shape
+        if meta_path.exists():
+            meta = json.loads(meta_path.read_text())
+            ns, nt = meta.get("n_samples"), meta.get("n_traces")
+            if ns and nt and tuple(self._z.shape) == (ns, nt):
+                self._transposed = True
+                self._n_samples, self._n_traces = ns, nt
+
+    def read_traces(self, trace_numbers: np.ndarray) -> np.ndarray:
+        idx = np.asarray(trace_numbers, np.int64)
+        return self._z.read(idx).T if self._transposed else self._z.read_rows(idx)
+
+    def get_n_samples(self) -> int:
+        return self._n_samples
+
+    @property
+    def n_traces(self) -> int:
+        return self._n_traces
+
+    @property
+    def shape(self):
+        return (self._n_traces, self._n_samples)
+
+    @property
+    def is_transposed(self) -> bool:
+        return self._transposed
 
 
 class TraceUpload:

@@ -69,8 +69,8 @@ class PSTMPlan:
     float32.  ``forward_only=True`` is for plans that only migrate: float32
     traces are staged in intercept form (one FMA per interpolation tap, ~3 %
     faster); ``demigrate`` then matches the migration's transpose to ~1e-5
-    rather than to float rounding, and ``velocity_gradient`` and batches refuse
-    the plan.  ``taper_width`` in (0, 1) adds the aperture controller's
+    rather than to float rounding, and ``velocity_gradient`` refuses the plan
+    (a batch takes it when all of its class plans are forward_only).  ``taper_width`` in (0, 1) adds the aperture controller's
     distance and angle cosine tapers of both legs (migration only, float32).
     ``ray_gradient`` k != 0 takes curved-ray traveltimes in v(z) = v0 + k z
     (the velocity passed is v0), as the reference migrator's default table.

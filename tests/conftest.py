@@ -10,6 +10,13 @@ if ROOT not in sys.path:
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
+# the kernel-shape tuner's cache: one file per test session, inherited by the
+# subprocesses the tests start, never the user's
+import tempfile  # noqa: E402
+
+os.environ.setdefault("SEISPSTM_TUNE_CACHE",
+                      os.path.join(tempfile.gettempdir(), f"seispstm_tune_tests_{os.getpid()}.json"))
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA (B200) device and libseispstm.so")

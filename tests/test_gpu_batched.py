@@ -9,7 +9,7 @@ from conftest import rel_l2
 pytestmark = pytest.mark.gpu
 
 
-def _classes(storage="f32"):
+def _classes(storage="f32", forward_only=False):
     from seisproc_b200 import synthetic
     from seisproc_b200.kirchhoff import PSTMPlan
     surveys = synthetic.survey_classes([900, 300, 1500, 50], seed=3, n_offset_bins=2,
@@ -26,15 +26,19 @@ def _classes(storage="f32"):
                               il_dy=0.0, xl_dx=0.0, xl_dy=s.xl_spacing, t0_ms=0.0,
                               dt_ms=s.dt_ms, n_samples=s.n_samples, in_t0_ms=0.0,
                               in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
-                              max_angle_deg=s.max_angle_deg, storage=storage))
+                              max_angle_deg=s.max_angle_deg, storage=storage,
+                              forward_only=forward_only))
     v = torch.from_numpy(surveys[0].vrms).to(dev)
     return surveys, plans, v
 
 
-@pytest.mark.parametrize("storage", ["f32", "bf16"])
-def test_batched_matches_per_class_plans(storage):
+@pytest.mark.parametrize("storage,forward_only", [("f32", False), ("f32", True), ("bf16", False),
+                                                  ("bf16", True)])
+def test_batched_matches_per_class_plans(storage, forward_only):
+    """Forward_only float32 class plans run the batched kernel over
+    intercept-form rows, the others over (x, dx) or 16-bit rows."""
     from seisproc_b200.batched import BatchedPSTM
-    surveys, plans, v = _classes(storage)
+    surveys, plans, v = _classes(storage, forward_only)
     traces = [s.traces.cuda() for s in surveys]
     b = BatchedPSTM(plans, v)
     b.load(traces)
@@ -67,7 +71,7 @@ def test_batched_graph_replay_follows_inputs():
 
 def test_autotuner_picks_and_caches(tmp_path, monkeypatch):
     from seisproc_b200 import autotune
-    monkeypatch.setattr(autotune, "_CACHE_PATH", str(tmp_path / "tune.json"))
+    monkeypatch.setenv("SEISPSTM_TUNE_CACHE", str(tmp_path / "tune.json"))
     surveys, plans, v = _classes()
     s = surveys[2]
     p0 = plans[2]
@@ -128,3 +132,102 @@ def test_from_survey_matches_per_class_plans():
         assert torch.equal(img, ri) and torch.equal(fold, rf)
         p.close()
     b.close()
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+def test_engine_migrate_bins_full_matches_per_bin_calls(storage):
+    """MigrationEngine.migrate_bins_full (every bin in one batched launch) gives
+    each bin the image and fold that migrate_bin_full gives it alone, into new
+    arrays or into the caller's page-locked buffers."""
+    from seisproc_b200.engine import MigrationEngine
+    surveys, plans, v = _classes(storage)
+    for p in plans:
+        p.close()
+    s0 = surveys[0]
+    kw = dict(origin_x=s0.origin_x, origin_y=s0.origin_y, il_spacing=s0.il_spacing,
+              xl_spacing=s0.xl_spacing, azimuth_deg=0.0, n_il=s0.n_il, n_xl=s0.n_xl,
+              dt_ms=s0.dt_ms, t_min_ms=0.0, n_times=s0.n_times,
+              max_aperture_m=s0.max_aperture_m, max_angle_deg=s0.max_angle_deg,
+              velocity_model=s0.vrms)
+    eng = MigrationEngine(storage=storage)
+    bins = [{"traces": s.traces.cpu().numpy(), "source_x": s.source_x, "source_y": s.source_y,
+             "receiver_x": s.receiver_x, "receiver_y": s.receiver_y} for s in surveys]
+    res = eng.migrate_bins_full(bins, **kw)
+    shape = (s0.n_times, s0.n_il, s0.n_xl)
+    outs = [(torch.empty(shape, pin_memory=True), torch.empty(shape, pin_memory=True))
+            for _ in bins]
+    res2 = eng.migrate_bins_full(bins, out=outs, **kw)
+    for b, (img, fold), (img2, fold2) in zip(bins, res, res2):
+        ri, rf = eng.migrate_bin_full(b["traces"], b["source_x"], b["source_y"],
+                                      b["receiver_x"], b["receiver_y"], **kw)
+        assert img.shape == ri.shape and fold.shape == rf.shape
+        assert rel_l2(img, ri) <= 1e-6 and np.array_equal(fold, rf)
+        assert np.array_equal(img2.numpy(), img) and np.array_equal(fold2.numpy(), fold)
+
+
+def test_autotuner_choice_is_used_and_cached(tmp_path, monkeypatch):
+    """choose_variant times the candidate shapes (256- and 128-sample windows
+    among them) on a crop, caches the winner under the device and library
+    ABI, and the engine builds its plans with that shape; a second choice is a
+    cache hit that times nothing."""
+    import json
+    from seisproc_b200 import autotune
+    from seisproc_b200.engine import MigrationEngine
+    cache = tmp_path / "tune.json"
+    monkeypatch.setenv("SEISPSTM_TUNE_CACHE", str(cache))
+    surveys, plans, v = _classes()
+    for p in plans:
+        p.close()
+    s = surveys[2]
+    dev = torch.device("cuda")
+    coords = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+              for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    kw = dict(n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+              origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0, xl_dy=s.xl_spacing,
+              t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples, in_t0_ms=0.0, in_dt_ms=s.dt_ms,
+              max_aperture_m=s.max_aperture_m, max_angle_deg=s.max_angle_deg, forward_only=True)
+    best = autotune.choose_variant(coords, velocity=v, **kw)
+    d = json.loads(cache.read_text())
+    (tag, entries), = d.items()
+    assert tag == autotune.device_tag()
+    (key, entry), = entries.items()
+    assert entry["variant"] == best and set(map(int, entry["ms"])) == set(autotune.GRID_SHAPES)
+    assert {10, 11} <= set(autotune.GRID_SHAPES)
+    mtime = cache.stat().st_mtime_ns
+    assert autotune.choose_variant(coords, velocity=v, **kw) == best
+    assert cache.stat().st_mtime_ns == mtime  # a hit writes nothing
+    eng = MigrationEngine()
+    eng.migrate_bin_full(s.traces.cpu().numpy(), s.source_x, s.source_y, s.receiver_x,
+                         s.receiver_y, s.origin_x, s.origin_y, s.il_spacing, s.xl_spacing, 0.0,
+                         s.n_il, s.n_xl, s.dt_ms, 0.0, s.n_times, max_aperture_m=s.max_aperture_m,
+                         max_angle_deg=s.max_angle_deg, velocity_model=s.vrms)
+    assert eng.last_stats["variant"] == best
+
+
+@pytest.mark.parametrize("shape", [10, 11])
+def test_short_window_shapes_match_default_shape(shape):
+    """The 256- and 128-sample windows give the fold of the 512-sample shape
+    exactly and its image to float rounding: each window stages its rows from
+    its own first sample, and that offset enters the float32 sample index, so
+    the fractional parts round differently (measured 2.4e-6)."""
+    surveys, plans, v = _classes()
+    from seisproc_b200.kirchhoff import PSTMPlan
+    s = surveys[2]
+    dev = torch.device("cuda")
+    c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    kw = dict(n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+              origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0, xl_dy=s.xl_spacing,
+              t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples, in_t0_ms=0.0, in_dt_ms=s.dt_ms,
+              max_aperture_m=s.max_aperture_m, max_angle_deg=s.max_angle_deg)
+    ref = PSTMPlan(*c, variant=3, **kw)
+    alt = PSTMPlan(*c, variant=shape, **kw)
+    ri, rf = ref.migrate(s.traces.cuda(), v)
+    ai, af = alt.migrate(s.traces.cuda(), v)
+    ref.check()
+    alt.check()
+    assert alt.stats()["t_window"] == {10: 256, 11: 128}[shape]
+    assert torch.equal(af, rf)
+    assert rel_l2(ai.cpu().numpy(), ri.cpu().numpy()) <= 1e-5
+    for p in plans + [ref, alt]:
+        p.close()

@@ -22,7 +22,7 @@ def _kw(s):
 
 
 @pytest.mark.parametrize("blocks", [1, 3])
-@pytest.mark.parametrize("kind", ["numpy", "segy"])
+@pytest.mark.parametrize("kind", ["numpy", "segy", "zarr"])
 def test_reader_path_equals_array_path(tmp_path, kind, blocks):
     from seisproc_b200 import ingest as I
     from seisproc_b200 import velocity_io as V
@@ -31,10 +31,20 @@ def test_reader_path_equals_array_path(tmp_path, kind, blocks):
     tr_major = np.ascontiguousarray(s.traces.cpu().numpy().T)  # (n_traces, n_samples)
     if kind == "numpy":
         reader = I.NumpyDataReader(tr_major)
-    else:
+    elif kind == "segy":
         p = tmp_path / "bin.sgy"
         V.write_segy_traces(p, tr_major, int(s.dt_ms * 1000), fmt=5)
         reader = I.SegyDataReader(p)
+    else:
+        # the reference import's layout: (n_samples, n_traces) beside metadata.json
+        import json
+        from seisproc_b200.output_storage import ZarrV2Array
+        ZarrV2Array.create(tmp_path / "traces.zarr", tr_major.T.shape, (s.n_samples, 1000)
+                           ).write(np.ascontiguousarray(tr_major.T))
+        (tmp_path / "metadata.json").write_text(json.dumps(
+            {"n_samples": s.n_samples, "n_traces": s.n_traces}))
+        reader = I.ZarrDataReader(tmp_path)
+        assert reader.is_transposed
     rs = np.random.RandomState(3)
     idx = np.sort(rs.choice(s.n_traces, 3700, replace=False))  # one bin's traces
     coords = [np.asarray(a)[idx] for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]

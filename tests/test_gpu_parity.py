@@ -69,6 +69,36 @@ def test_full_2d_config_matches_reference():
     assert flips <= FOLD_FLIP_FRAC * ref["fold"].sum(), flips
 
 
+def test_full_3d_20k_matches_reference():
+    """20k traces x 500 samples -> 16 x 16 x 500 (golden made by running the
+    reference's migrate_bin_full at constant V; input regenerated from its
+    seed on the CPU and SHA-256 pinned)."""
+    import hashlib
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import survey_3d_20k
+    ref = load_golden("full_3d_20k")
+    s = survey_3d_20k()
+    tr = s.traces.numpy()
+    assert hashlib.sha256(tr.astype(np.float32).tobytes()).hexdigest() == str(ref["input_sha256"])
+    # 16-bit storage: the rounding of the stored samples (bf16 keeps 8
+    # significant bits, f16 11 with a per-trace scale) sets the error
+    for storage, tol in (("f32", FP32_TOL), ("bf16", 2e-3), ("f16", 3e-4)):
+        from seisproc_b200.engine import MigrationEngine
+        img, fold = MigrationEngine(storage=storage).migrate_bin_full(
+            traces=tr, source_x=s.source_x, source_y=s.source_y, receiver_x=s.receiver_x,
+            receiver_y=s.receiver_y, origin_x=s.origin_x, origin_y=s.origin_y,
+            il_spacing=s.il_spacing, xl_spacing=s.xl_spacing, azimuth_deg=0.0, n_il=s.n_il,
+            n_xl=s.n_xl, dt_ms=s.dt_ms, t_min_ms=0.0, n_times=s.n_times,
+            velocity_mps=s.velocity_mps, max_aperture_m=s.max_aperture_m,
+            max_angle_deg=s.max_angle_deg, normalize=False)
+        err = rel_l2(img, ref["image"])
+        flips = np.abs(fold - ref["fold"]).sum()
+        assert err <= tol, (storage, err)
+        assert flips <= max(2, FOLD_FLIP_FRAC * ref["fold"].sum()), (storage, flips)
+
+
 def _small_3d(seed=3, n_traces=4000, lateral=True, utm=(0.0, 0.0), n_samples=200):
     from seisproc_b200 import synthetic
     return synthetic.survey_3d(n_traces=n_traces, seed=seed, n_samples=n_samples, extent=1600.0,
@@ -248,24 +278,36 @@ def test_forward_only_low_clamp_and_16bit():
     assert np.array_equal(b1, b0)
 
 
-def test_forward_only_plan_refuses_gradient_and_batch():
+def test_forward_only_plan_refuses_gradient_and_mixed_batch():
+    """A forward_only plan has no V-gradient, and a batch takes it only with
+    other forward_only plans (the rows' form is one per launch)."""
     from seisproc_b200.batched import BatchedPSTM
     from seisproc_b200.kirchhoff import PSTMPlan
     s = _small_3d(seed=8, n_traces=1000)
     dev = torch.device("cuda")
     c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
          for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
-    plan = PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
-                    origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
-                    xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
-                    in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
-                    max_angle_deg=s.max_angle_deg, forward_only=True)
+
+    def make(fo):
+        return PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+                        origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                        xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                        in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                        max_angle_deg=s.max_angle_deg, forward_only=fo)
+    plan, other = make(True), make(False)
     v = torch.from_numpy(s.vrms).to(dev)
     img, _ = plan.migrate(s.traces.to(dev), v)
     with pytest.raises(Exception, match="forward_only"):
         plan.velocity_gradient(img, v)
+    other.load_traces(s.traces.to(dev))
     with pytest.raises(Exception, match="forward_only"):
-        BatchedPSTM([plan], v)
+        BatchedPSTM([plan, other], v)
+    b = BatchedPSTM([plan], v)
+    b.migrate()
+    b.check()
+    assert torch.equal(b.images[0], img)
+    b.close()
+    other.close()
     d = plan.demigrate(img, v)  # still the adjoint, to ~1e-5
     assert d.shape == s.traces.shape
     plan.check()

@@ -147,3 +147,64 @@ def test_two_rank_gather_and_cgls_match_one_process(tmp_path):
     assert np.allclose(got["res"], res1, rtol=1e-9)
     assert np.linalg.norm(got["m"] - m1.numpy()) <= 1e-9 * np.linalg.norm(m1.numpy())
     assert res1[-1] < 0.8  # the iterations reduce the misfit
+
+
+# --- bench.py's sharded mode (one survey, inline slabs over the ranks) -------
+
+def _bench_rank_main(rank, world, port, out_dir):
+    """One CPU rank of bench.py's sharded mode: the partition of one survey and
+    the whole-job aggregation (slowest rank's time, all ranks' pairs); the
+    rank's pairs come from the FP64 pair counter on its slab's columns."""
+    import json
+    import sys
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+        import bench
+        from seisproc_b200 import synthetic
+        s = synthetic.survey_3d(n_traces=3000, seed=9, n_samples=60, extent=900.0,
+                                max_offset=700.0, n_il=9, n_xl=5, spacing=25.0,
+                                n_diffractors=3, aperture=300.0, lateral_velocity=False)
+        slabs, halos = bench.shard_partition(s, world)
+        il0, il1 = slabs[rank]
+        halo = halos[rank]
+        il = np.arange(il0, il1)[:, None]
+        xl = np.arange(s.n_xl)[None, :]
+        cx = (s.origin_x + il * s.il_spacing + 0 * xl).ravel()
+        cy = (s.origin_y + 0 * il + xl * s.xl_spacing).ravel()
+        t_ms = np.arange(s.n_times) * s.dt_ms
+        pairs_halo = O.count_pairs_fp64(s.source_x[halo], s.source_y[halo], s.receiver_x[halo],
+                                        s.receiver_y[halo], cx, cy, t_ms, 2000.0,
+                                        s.max_aperture_m, s.max_angle_deg)
+        pairs_all = O.count_pairs_fp64(s.source_x, s.source_y, s.receiver_x, s.receiver_y, cx,
+                                       cy, t_ms, 2000.0, s.max_aperture_m, s.max_angle_deg)
+        ms, total = bench.shard_aggregate(10.0 + rank, float(pairs_halo), torch.device("cpu"))
+        with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
+            json.dump({"slabs": slabs, "halo": int(halo.size), "n": s.n_traces,
+                       "pairs_halo": float(pairs_halo), "pairs_all": float(pairs_all),
+                       "ms": ms, "total": total}, f)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_sharded_partition_and_aggregate_two_ranks(tmp_path):
+    """bench.py --gpus 2 (sharded mode) on two gloo ranks: the slabs tile the
+    inlines, each halo holds every pair of its slab (the culling loses none),
+    and the whole-job figures are the slowest rank's time and the sum of the
+    ranks' pairs, identical on both ranks."""
+    import json
+    world = 2
+    mp.start_processes(_bench_rank_main, args=(world, _free_port(), str(tmp_path)),
+                       nprocs=world, join=True, start_method="spawn")
+    r = [json.load(open(tmp_path / f"rank{i}.json")) for i in range(world)]
+    assert r[0]["slabs"] == r[1]["slabs"] == [[0, 5], [5, 9]]
+    for x in r:
+        assert x["pairs_halo"] == x["pairs_all"] > 0
+        assert x["halo"] < x["n"]
+    assert r[0]["ms"] == r[1]["ms"] == 11.0
+    assert r[0]["total"] == r[1]["total"] == r[0]["pairs_halo"] + r[1]["pairs_halo"]
