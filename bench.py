@@ -969,6 +969,44 @@ def bench_lsq(args):
         an.append(float((vv.grad.double() * dv.double()).sum()))
     fd, an = np.array(fd), np.array(an)
     plan.check()
+    # the same geometry with band-limited noise-free data (8 Hz) and output
+    # times from 200 ms: the forward map is smooth in V except at the linear
+    # interpolation's sample kinks, so the finite differences should agree with
+    # the gradient kernel to ~1e-2 (criterion); the noisy 30 Hz workload above
+    # also crosses mask switches and kinks within the step
+    sm = synthetic.survey_3d(n_traces=args.lsq_traces, seed=7, device=dev, n_samples=500,
+                             dt_ms=2.0, extent=2500.0, max_offset=1500.0, n_il=100, n_xl=100,
+                             spacing=25.0, n_diffractors=60, aperture=1000.0, f_peak=8.0,
+                             noise_rel=0.0, n_times=400)
+    cs = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+          for a in (sm.source_x, sm.source_y, sm.receiver_x, sm.receiver_y)]
+    # an 89 deg angle limit: the aperture mask does not depend on V, so no mask
+    # switches under the perturbation (the gradient holds the masks fixed)
+    psm = PSTMPlan(*cs, n_il=sm.n_il, n_xl=sm.n_xl, n_times=400, origin_x=sm.origin_x,
+                   origin_y=sm.origin_y, il_dx=sm.il_spacing, il_dy=0.0, xl_dx=0.0,
+                   xl_dy=sm.xl_spacing, t0_ms=200.0, dt_ms=sm.dt_ms, n_samples=sm.n_samples,
+                   in_t0_ms=0.0, in_dt_ms=sm.dt_ms, max_aperture_m=sm.max_aperture_m,
+                   max_angle_deg=89.0)
+    vs = torch.from_numpy(sm.vrms).to(dev)
+    gs = torch.randn(vs.shape, device=dev, generator=torch.Generator(device=dev).manual_seed(4))
+    vsg = vs.clone().requires_grad_(True)
+    (migrate(sm.traces, vsg, psm) * gs).sum().backward()
+    rs2 = np.random.RandomState(21)
+    fd2, an2 = [], []
+    t2 = np.linspace(0.0, 1.0, 400)[:, None, None]
+    for _ in range(args.fd_directions):
+        # smooth random direction (V t0 stays increasing in t0)
+        c = rs2.randn(4)
+        f = (c[0] + c[1] * np.sin(np.pi * (t2 + rs2.rand())) + c[2] * np.cos(2 * np.pi * xx)
+             + c[3] * np.sin(2 * np.pi * yy))
+        dv = torch.from_numpy((f / np.abs(f).max()).astype(np.float32)).to(dev) * vs * 1e-3
+        f2_ = lambda x: float((migrate(sm.traces, x, psm).double() * gs.double()).sum())
+        fd2.append((f2_(vs + dv) - f2_(vs - dv)) / 2.0)
+        an2.append(float((vsg.grad.double() * dv.double()).sum()))
+    fd2, an2 = np.array(fd2), np.array(an2)
+    psm.check()
+    psm.close()
+    del sm, cs
     d = plan.demigrate(migrate(tr, v, plan), v)  # data in the range of L
     m, hist = cgls(plan, d, v, n_iter=args.cg_iters)
     it_s = [h[2] for h in hist[1:]]
@@ -984,6 +1022,13 @@ def bench_lsq(args):
                      if args.fd_directions else None,
                      "note": "noisy 30 Hz data from t0 = 0: includes interpolation kinks and "
                              "mask switches"},
+        "vgrad_fd_smooth": {"directions": args.fd_directions,
+                            "rel_l2": float(np.linalg.norm(fd2 - an2) / np.linalg.norm(fd2))
+                            if args.fd_directions else None, "criterion": 1e-2,
+                            "note": "same geometry and size, 8 Hz noise-free data, output "
+                                    "times 200-998 ms, 1000 m aperture with an 89 deg angle "
+                                    "limit (no V-dependent mask), smooth random "
+                                    "perturbations of relative size 1e-3"},
         "cg": {"residual_history": [h[1] for h in hist], "misfit_reduction": hist[-1][1]},
     }), flush=True)
     plan.close()
@@ -1367,9 +1412,11 @@ def main():
     ap.add_argument("--aa-lmax", type=float, default=32.0)
     ap.add_argument("--utm", action="store_true",
                     help="world coordinates offset by a UTM origin (5e5, 6e6) m")
-    ap.add_argument("--shard-mode", default="slabs", choices=["slabs", "replicas"],
-                    help="with N > 1 ranks: inline slabs of one survey (strong scaling) or one "
-                         "independent survey per rank (weak scaling)")
+    ap.add_argument("--shard-mode", default="auto", choices=["auto", "slabs", "replicas"],
+                    help="auto: inline slabs of one survey when N > 1 ranks (strong scaling), "
+                         "the single-plan path on one; slabs: the slab path at any N (one "
+                         "slab = the whole grid on one rank); replicas: one independent "
+                         "survey per rank (weak scaling)")
     ap.add_argument("--classes", type=int, default=64,
                     help="batched config: the first N of the 64 offset/azimuth classes")
     ap.add_argument("--lsq-traces", type=int, default=120_000)
@@ -1393,7 +1440,8 @@ def main():
         return bench_time_rms(args) if args.impl == "ours" else bench_time_rms_reference(args)
     if args.impl == "reference":
         bench_reference(args)
-    elif int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.shard_mode == "slabs":
+    elif args.shard_mode == "slabs" or (args.shard_mode == "auto" and
+                                         int(os.environ.get("WORLD_SIZE", "1")) > 1):
         bench_sharded(args)
     else:
         bench_ours(args)

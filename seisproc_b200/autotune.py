@@ -2,7 +2,8 @@
 
 A kernel shape fixes the output tile (columns per CTA, tile_il x tile_xl) and
 the time window per CTA (warps per column x 64 x groups per lane): 1024, 512,
-256 or 128 output samples.  For a problem the tuner builds a plan per candidate
+256 or 128 output samples.  Shapes of 256 threads run two CTAs per SM, each
+with half the shared memory.  For a problem the tuner builds a plan per candidate
 shape on a centred crop of the output grid (at most 32 x 32 columns, all output
 times, the traces within reach of the crop), times the forward migration with
 CUDA events and keeps the fastest.  The kernel's run time depends on the
@@ -43,9 +44,10 @@ SHAPES: Dict[int, Tuple[int, int, int, int]] = {
     10: (16, 4, 4, 256),
     11: (16, 4, 4, 128),
     12: (16, 16, 1, 256),
+    13: (8, 2, 4, 512),
 }
 LINE_SHAPES = (5, 6, 7, 8, 9, 12)
-GRID_SHAPES = (1, 2, 3, 4, 10, 11)
+GRID_SHAPES = (1, 2, 3, 4, 10, 11, 13)
 CROP = 32  # columns per crop side
 
 _lock = threading.Lock()
@@ -127,7 +129,10 @@ def tune(make_plan: Callable[[int], "object"], traces: torch.Tensor, velocity, k
             return v, {}
     times = {}
     for var in variants:
-        plan = make_plan(var)
+        try:
+            plan = make_plan(var)
+        except (ValueError, NotImplementedError):
+            continue  # e.g. traces too long for this shape's shared-memory ring
         try:
             plan.load_traces(traces)
             plan.migrate_loaded(velocity, with_fold=False)  # warm-up

@@ -296,6 +296,7 @@ cudaError_t adj_dispatch(const Plan* p, const KArgs& A, const float4* tab, cudaS
   switch (p->shape.id) {
     case 1:
     case 5:
+    case 13:
       return adj_wm<8, 2, 8>(p, A, tab, s);
     case 2:
     case 8:

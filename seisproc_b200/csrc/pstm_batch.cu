@@ -119,6 +119,8 @@ cudaError_t batch_dispatch(const Batch* b, cudaStream_t s) {
       return batch_st<16, 1, 4>(b, s);
     case 11:
       return batch_st<16, 1, 2>(b, s);
+    case 13:
+      return batch_st<8, 1, 8>(b, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -187,7 +189,7 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
   b->vst = v_stride_t;
   b->vsc = v_stride_c;
   if (!ring_shape(p0->shape.cols, p0->shape.t_window(), p0->row_stride, p0->elt_bytes,
-                  &b->ring_stages, &b->ring_rows)) {
+                  &b->ring_stages, &b->ring_rows, smem_budget(p0->shape.threads()))) {
     free_batch(b);
     return bfail(PSTM_EINVAL, "traces too long for the staged kernel");
   }

@@ -25,6 +25,16 @@ constexpr int kMaxStages = 4;
 constexpr int kRowGuard = 16;
 constexpr int kSmemBudget = 227 * 1024;
 
+// CTAs per SM a kernel shape is built for: 256-thread CTAs run two per SM
+// (128 registers each, half the shared-memory ring each), so one CTA's stage
+// waits overlap the other's sweeps; 512-thread CTAs run one.
+__host__ __device__ constexpr int ctas_per_sm(int threads) { return threads <= 256 ? 2 : 1; }
+// Dynamic shared memory one CTA of the shape may take (the SM's 228 KB shared
+// by its CTAs, less the 1 KB the hardware reserves per CTA).
+__host__ __device__ constexpr int smem_budget(int threads) {
+  return ctas_per_sm(threads) == 1 ? kSmemBudget : (228 * 1024) / 2 - 1024;
+}
+
 struct Smem2 {
   int bars, thr, hist, raw, total;
 };
@@ -49,10 +59,11 @@ __host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, i
 // Ring of the largest stages (up to 32 rows), then the most stages (up to 4,
 // at least 2), that fits: large stages measured faster than deeper rings of
 // smaller ones (fewer barrier round trips per trace).
-inline bool ring_shape(int cols, int T, int S, int elt, int* stages, int* sb) {
+inline bool ring_shape(int cols, int T, int S, int elt, int* stages, int* sb,
+                       int budget = kSmemBudget) {
   for (int b = kBlockTraces; b >= 1; b >>= 1)
     for (int st = kMaxStages; st >= 2; --st)
-      if (smem2_layout(cols, T, S, elt, st, b).total <= kSmemBudget) {
+      if (smem2_layout(cols, T, S, elt, st, b).total <= budget) {
         *stages = st;
         *sb = b;
         return true;
@@ -690,7 +701,8 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
 
 template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP, bool AA = false,
           bool TAPER = false, bool CURVED = false>
-__global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const KArgs A) {
+__global__ void __launch_bounds__(COLS* WPC * 32, ctas_per_sm(COLS* WPC * 32))
+    pstm_gather2_kernel(const KArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   gather_tile<COLS, WPC, M, ST, WM, LOWC, OP, AA, TAPER, CURVED>(A, blockIdx.x, blockIdx.y, smem);
 }
@@ -699,7 +711,7 @@ __global__ void __launch_bounds__(COLS* WPC * 32, 1) pstm_gather2_kernel(const K
 // device queue (items ordered by descending trace-list length) until none is
 // left.  Each class has its own plan data and output image in descs[class].
 template <int COLS, int WPC, int M, typename ST, int WM, bool LOWC, int OP>
-__global__ void __launch_bounds__(COLS* WPC * 32, 1)
+__global__ void __launch_bounds__(COLS* WPC * 32, ctas_per_sm(COLS* WPC * 32))
     pstm_batch_kernel(const KArgs* __restrict__ descs, const int4* __restrict__ items, int n_items,
                       int* __restrict__ counter) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -733,7 +745,8 @@ inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
                   : pstm_gather2_kernel<COLS, WPC, M, ST, WM, false, OP, AA, TAPER, CURVED>;
   const int T = WPC * 64 * M;
   KArgs A2 = A;
-  if (!ring_shape(COLS, T, p->row_stride, (int)sizeof(ST), &A2.ring_stages, &A2.ring_rows))
+  if (!ring_shape(COLS, T, p->row_stride, (int)sizeof(ST), &A2.ring_stages, &A2.ring_rows,
+                  smem_budget(COLS * WPC * 32)))
     return cudaErrorInvalidValue;
   const Smem2 L = smem2_layout(COLS, T, p->row_stride, (int)sizeof(ST), A2.ring_stages,
                                A2.ring_rows);
@@ -840,6 +853,8 @@ inline cudaError_t dispatch2_shape(const Plan* p, const KArgs& A, cudaStream_t s
       return dispatch2_st<16, 1, 4, OP>(p, A, s);
     case 11:
       return dispatch2_st<16, 1, 2, OP>(p, A, s);
+    case 13:
+      return dispatch2_st<8, 1, 8, OP>(p, A, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -26,6 +26,8 @@ cudaError_t launch_forward_icpt(const Plan* p, const KArgs& A, cudaStream_t s) {
       return dispatch2_wm<16, 1, 4, RowIcpt, OP_FWD>(p, A, s);
     case 11:
       return dispatch2_wm<16, 1, 2, RowIcpt, OP_FWD>(p, A, s);
+    case 13:
+      return dispatch2_wm<8, 1, 8, RowIcpt, OP_FWD>(p, A, s);
   }
   return cudaErrorInvalidValue;
 }

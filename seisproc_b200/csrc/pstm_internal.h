@@ -79,6 +79,7 @@ bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out);
 // pstm_test_set_injection); always 0 in the product build.
 int test_injection();
 size_t forward_smem_bytes(const Plan* p);
+size_t forward_smem_budget(const Plan* p);  // per-CTA shared memory of the plan's shape
 void count_launch();
 // Device memory of plans and their temporaries: stream-ordered allocations from
 // a library pool per device that keeps up to kPoolKeepBytes of freed memory

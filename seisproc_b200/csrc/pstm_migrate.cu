@@ -148,6 +148,7 @@ static const Shape kShapes[] = {
     {10, 16, 1, 4, 4, 4},  // 16 columns (4x4) x 256 samples
     {11, 16, 1, 2, 4, 4},  // 16 columns (4x4) x 128 samples
     {12, 16, 1, 4, 16, 1},  // 2D lines: 16 inlines x 256 samples
+    {13, 8, 1, 8, 2, 4},  // 8 columns (2x4) x 512 samples, 8 warps, two CTAs per SM
 };
 
 bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out) {
@@ -167,6 +168,8 @@ bool shape_for_variant(int variant, int n_xl, int n_times, Shape* out) {
   }
   return false;
 }
+
+size_t forward_smem_budget(const Plan* p) { return (size_t)smem_budget(p->shape.threads()); }
 
 size_t forward_smem_bytes(const Plan* p) {
   // pipelined forward kernel: the smallest ring (2 stages x 1 row) must fit

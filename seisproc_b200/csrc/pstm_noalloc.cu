@@ -246,7 +246,7 @@ extern "C" pstm_status pstm_migrate_noalloc(const pstm_grid* grid, const pstm_pa
   p.xl_dx = (float)grid->xl_dx;
   p.xl_dy = (float)grid->xl_dy;
   p.tan_theta = (float)std::tan(params->max_angle_deg * M_PI / 180.0);
-  if (forward_smem_bytes(&p) > 227 * 1024)
+  if (forward_smem_bytes(&p) > forward_smem_budget(&p))
     return noalloc_fail(PSTM_EINVAL, "traces too long for the staged kernel");
 
   // scratch layout (worst case: every trace listed for every tile)

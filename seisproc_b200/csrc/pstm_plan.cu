@@ -769,7 +769,7 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
   p->xl_dy = (float)g->xl_dy;
   p->tan_theta = (float)std::tan(prm->max_angle_deg * M_PI / 180.0);
   const size_t smem = forward_smem_bytes(p);
-  if (smem > 227 * 1024)
+  if (smem > forward_smem_budget(p))
     return fail(PSTM_EINVAL, "traces too long for the staged kernel (" +
                                  std::to_string(prm->n_samples) + " samples)");
   CUDA_TRY(dalloc(p, &p->err, 4, s));
