@@ -31,6 +31,7 @@ struct Batch {
   int* d_counter = nullptr;
   int n_items = 0;
   int ring_stages = 0, ring_rows = 0;
+  int hist16 = 0;  // 16-bit fold histogram: every class's tile lists < 65536 traces
   int sms = 0;
 };
 
@@ -44,7 +45,8 @@ cudaError_t launch_batch_one(const Batch* b, cudaStream_t s) {
   auto kern = pstm_batch_kernel<COLS, WPC, M, ST, WM, LC, OP_FWD>;
   const Plan* p = b->plans[0];
   const int T = WPC * 64 * M;
-  const Smem2 L = smem2_layout(COLS, T, p->row_stride, (int)sizeof(ST), b->ring_stages, b->ring_rows);
+  const Smem2 L = smem2_layout(COLS, T, p->row_stride, (int)sizeof(ST), b->ring_stages, b->ring_rows,
+                               hist_entry_bytes(b->hist16 != 0));
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total);
   if (e != cudaSuccess) return e;
   int per_sm = 1;
@@ -188,8 +190,12 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
   b->vel = velocity;
   b->vst = v_stride_t;
   b->vsc = v_stride_c;
+  b->hist16 = 1;
+  for (const Plan* p : b->plans)
+    if (p->longest_list >= 65536) b->hist16 = 0;
   if (!ring_shape(p0->shape.cols, p0->shape.t_window(), p0->row_stride, p0->elt_bytes,
-                  &b->ring_stages, &b->ring_rows, smem_budget(p0->shape.threads()))) {
+                  &b->ring_stages, &b->ring_rows, smem_budget(p0->shape.threads()),
+                  hist_entry_bytes(b->hist16 != 0))) {
     free_batch(b);
     return bfail(PSTM_EINVAL, "traces too long for the staged kernel");
   }
@@ -206,6 +212,7 @@ pstm_status pstm_batch_create(pstm_batch** out, pstm_plan* const* plans, int32_t
     descs[i].fold_out = b->folds[i];  // fold counted in the same launch (or nullptr)
     descs[i].ring_stages = b->ring_stages;
     descs[i].ring_rows = b->ring_rows;
+    descs[i].hist16 = b->hist16;  // one shared-memory layout for every class
     std::vector<int64_t> off(p->n_tiles + 1);
     cudaError_t e = cudaMemcpyAsync(off.data(), p->tile_off, off.size() * sizeof(int64_t),
                                     cudaMemcpyDeviceToHost, s);

@@ -56,6 +56,7 @@ struct KArgs {
   float cr_k, cr_scale;
   long long n_traces;  // rows staged (bounds of the list entries)
   int inject;          // checked test build only: the fault to simulate (0 = none)
+  int hist16;          // fold histogram in 16-bit halves (every tile list < 65536 traces)
 };
 
 // Faults the checked test build can simulate (pstm_test_set_injection); the
@@ -251,6 +252,7 @@ inline KArgs make_args(const Plan* p, const float* vel, int64_t vst, int64_t vsc
   }
   A.n_traces = p->n_traces;
   A.inject = test_injection();
+  A.hist16 = p->longest_list < 65536 ? 1 : 0;
   A.cr_k = (float)p->params.ray_gradient;
   A.cr_scale = p->params.ray_gradient != 0
                    ? (float)(1000.0 / (p->params.ray_gradient * p->params.in_dt_ms))

@@ -38,8 +38,13 @@ __host__ __device__ constexpr int smem_budget(int threads) {
 struct Smem2 {
   int bars, thr, hist, raw, total;
 };
-// Ring of `stages` stages of `sb` trace rows each.
-__host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, int stages, int sb) {
+// Bytes per fold-histogram entry: 16-bit counts when every tile list is
+// shorter than 65536 traces (no count can exceed its list's length).
+inline int hist_entry_bytes(bool hist16) { return hist16 ? 2 : 4; }
+// Ring of `stages` stages of `sb` trace rows each; `hb` bytes per fold
+// histogram entry.
+__host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, int stages, int sb,
+                                              int hb = 4) {
   Smem2 L;
   int o = 0;
   L.bars = o;
@@ -48,7 +53,7 @@ __host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, i
   L.thr = o;
   o += cols * T * 4;
   L.hist = o;  // fold histogram of first contributing samples
-  o += cols * T * 4;
+  o += cols * T * hb;
   o = (o + 127) & ~127;
   L.raw = o;
   o += stages * sb * (S * elt + kRowGuard);
@@ -58,12 +63,16 @@ __host__ __device__ inline Smem2 smem2_layout(int cols, int T, int S, int elt, i
 
 // Ring of the largest stages (up to 32 rows), then the most stages (up to 4,
 // at least 2), that fits: large stages measured faster than deeper rings of
-// smaller ones (fewer barrier round trips per trace).
+// smaller ones (fewer barrier round trips per trace; on the 3D workload 2 x 10
+// rows ran 1 % faster than 2 x 8 and 3 x 8 slower than 2 x 8).  Stage sizes
+// other than 1 are even, so a stage's traces are always swept in pairs.
 inline bool ring_shape(int cols, int T, int S, int elt, int* stages, int* sb,
-                       int budget = kSmemBudget) {
-  for (int b = kBlockTraces; b >= 1; b >>= 1)
+                       int budget = kSmemBudget, int hb = 4) {
+  static_assert(kBlockTraces == 32, "one bulk copy per lane of warp 0");
+  static const int kRows[] = {32, 24, 16, 12, 10, 8, 6, 4, 2, 1};
+  for (const int b : kRows)
     for (int st = kMaxStages; st >= 2; --st)
-      if (smem2_layout(cols, T, S, elt, st, b).total <= budget) {
+      if (smem2_layout(cols, T, S, elt, st, b, hb).total <= budget) {
         *stages = st;
         *sb = b;
         return true;
@@ -252,39 +261,49 @@ __device__ __forceinline__ void sweep_traces(f2 (&acc)[M], const f2 (&zz)[M], co
   }
 }
 
-// A masked sweep (some trace starts inside the warp's segment) entered at g0,
-// the first group holding a contributing sample, through a jump table: the
-// groups from g0 on run as one straight-line block, each group masked by
-// sample index, with no per-group branch (measured 1.3 % faster than testing
-// every group against g0).
-#define PSTM_SWEEP_GROUP(I)                                                                     \
+// The sweep of a warp's M groups for NTR traces, entered through a jump table:
+// groups g0..g1 (g0 holding the earliest first contributing sample of the
+// traces, g1 the latest) masked by sample index, the groups after g1 plain
+// (every sample contributes); g1 < 0 runs every group plain.  One
+// straight-line block, no per-group branch in the plain part: against masking
+// every group from g0 on it issues 4.6 % fewer instructions (the sample masks'
+// compares and selects) and ran 0.8 % faster on the 3D workload.
+#define PSTM_SWEEP_GROUP(I, MK)                                                                 \
   if constexpr ((I) < M) {                                                                      \
-    sweep_traces<1, ST, WM, LOWC, true, OP, NTR, TAPER, CURVED>(                                \
+    sweep_traces<1, ST, WM, LOWC, MK, OP, NTR, TAPER, CURVED>(                                  \
         reinterpret_cast<f2(&)[1]>(acc[(I) % M]), reinterpret_cast<const f2(&)[1]>(zz[(I) % M]), \
         reinterpret_cast<const f2(&)[1]>(aa[(I) % M]), hs2, hr2, rbase, kst, sc, bb, magic2,     \
         hi_c, lo_c, kw + 64 * (I), lane, 0, tp, cr_scale, rc);                                  \
   }
 template <int M, typename ST, int WM, bool LOWC, int OP, int NTR, bool TAPER, bool CURVED>
-__device__ __forceinline__ void sweep_masked_from(f2 (&acc)[M], const f2 (&zz)[M],
-                                                  const f2 (&aa)[M], const float (&hs2)[NTR],
-                                                  const float (&hr2)[NTR],
-                                                  const uint32_t (&rbase)[NTR],
-                                                  const int (&kst)[NTR], const float (&sc)[NTR],
-                                                  f2 bb, f2 magic2, float hi_c, float lo_c, int kw,
-                                                  int lane, int g0, const TaperArgs& tp,
-                                                  float cr_scale, RowCheck rc) {
+__device__ __forceinline__ void sweep_split(f2 (&acc)[M], const f2 (&zz)[M], const f2 (&aa)[M],
+                                            const float (&hs2)[NTR], const float (&hr2)[NTR],
+                                            const uint32_t (&rbase)[NTR], const int (&kst)[NTR],
+                                            const float (&sc)[NTR], f2 bb, f2 magic2, float hi_c,
+                                            float lo_c, int kw, int lane, int g0, int g1,
+                                            const TaperArgs& tp, float cr_scale, RowCheck rc) {
   static_assert(M <= 8, "the jump table covers up to 8 groups");
+  if (g1 < 0) goto plain0;
   switch (g0 < 0 ? 0 : g0) {
-    case 0: PSTM_SWEEP_GROUP(0) [[fallthrough]];
-    case 1: PSTM_SWEEP_GROUP(1) [[fallthrough]];
-    case 2: PSTM_SWEEP_GROUP(2) [[fallthrough]];
-    case 3: PSTM_SWEEP_GROUP(3) [[fallthrough]];
-    case 4: PSTM_SWEEP_GROUP(4) [[fallthrough]];
-    case 5: PSTM_SWEEP_GROUP(5) [[fallthrough]];
-    case 6: PSTM_SWEEP_GROUP(6) [[fallthrough]];
-    case 7: PSTM_SWEEP_GROUP(7) [[fallthrough]];
-    default: break;
+    case 0: PSTM_SWEEP_GROUP(0, true) if (g1 <= 0) goto plain1; [[fallthrough]];
+    case 1: PSTM_SWEEP_GROUP(1, true) if (g1 <= 1) goto plain2; [[fallthrough]];
+    case 2: PSTM_SWEEP_GROUP(2, true) if (g1 <= 2) goto plain3; [[fallthrough]];
+    case 3: PSTM_SWEEP_GROUP(3, true) if (g1 <= 3) goto plain4; [[fallthrough]];
+    case 4: PSTM_SWEEP_GROUP(4, true) if (g1 <= 4) goto plain5; [[fallthrough]];
+    case 5: PSTM_SWEEP_GROUP(5, true) if (g1 <= 5) goto plain6; [[fallthrough]];
+    case 6: PSTM_SWEEP_GROUP(6, true) if (g1 <= 6) goto plain7; [[fallthrough]];
+    case 7: PSTM_SWEEP_GROUP(7, true) [[fallthrough]];
+    default: goto done;
   }
+plain0: PSTM_SWEEP_GROUP(0, false)
+plain1: PSTM_SWEEP_GROUP(1, false)
+plain2: PSTM_SWEEP_GROUP(2, false)
+plain3: PSTM_SWEEP_GROUP(3, false)
+plain4: PSTM_SWEEP_GROUP(4, false)
+plain5: PSTM_SWEEP_GROUP(5, false)
+plain6: PSTM_SWEEP_GROUP(6, false)
+plain7: PSTM_SWEEP_GROUP(7, false)
+done:;
 }
 #undef PSTM_SWEEP_GROUP
 
@@ -368,7 +387,8 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
   static_assert(kRowGuard % 16 == 0, "row data must stay 16-byte aligned");
   const int S = A.S;
   const int B = A.ring_rows, kStages = A.ring_stages;
-  const Smem2 L = smem2_layout(COLS, T, S, ES, kStages, B);
+  const bool h16 = A.hist16 != 0;
+  const Smem2 L = smem2_layout(COLS, T, S, ES, kStages, B, h16 ? 2 : 4);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);
   uint64_t* empty = full + kMaxStages;
   int* abort_flag = reinterpret_cast<int*>(empty + kMaxStages);
@@ -407,7 +427,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     float v = -1.0f;
     if (kk < nk && tile_column(A, tile, q, qil, qxl)) v = threshold(A, qil * A.n_xl + qxl, k0 + kk);
     thr[e] = v;
-    if (want_fold) hist[e] = 0;
+    if (want_fold && (!h16 || (e & 1) == 0)) hist[h16 ? e >> 1 : e] = 0;
   }
   __syncthreads();
 
@@ -519,7 +539,14 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         if (fv < nk) {
           ks = k0 + fv;
           // fold: one warp per column counts where each trace starts
-          if (want_fold && ts == 0) atomicAdd(hist + cl * T + fv, 1);
+          if (want_fold && ts == 0) {
+            // 16-bit counts: entry e is half e & 1 of word e / 2 (T is even)
+            const int e = cl * T + fv;
+            if (h16)
+              atomicAdd(reinterpret_cast<unsigned*>(hist) + (e >> 1), 1u << (16 * (e & 1)));
+            else
+              atomicAdd(hist + e, 1);
+          }
         }
         if constexpr (AA) {
           gxs = (xc - g_next.x) * A.aa_dx;
@@ -588,14 +615,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const float sc[2] = {__shfl_sync(0xffffffffu, tsc, t), __shfl_sync(0xffffffffu, tsc, t + 1)};
         const uint32_t rb[2] = {rb0, rb0 + (uint32_t)RP};
         const int kk[2] = {ka, kb};
-        if (ka > kw || kb > kw)
-          sweep_masked_from<M, ST, WM, LOWC, OP, 2, TAPER, CURVED>(
-              acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c, lo_c, kw, lane,
-              (min(ka, kb) - kw) >> 6, A.tp, A.cr_scale, rck);
-        else
-          sweep_traces<M, ST, WM, LOWC, false, OP, 2, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
-                                                              hi_c, lo_c, kw, lane, 0, A.tp,
-                                                              A.cr_scale, rck);
+        const int kmax = max(ka, kb);
+        sweep_split<M, ST, WM, LOWC, OP, 2, TAPER, CURVED>(
+            acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c, lo_c, kw, lane, (min(ka, kb) - kw) >> 6,
+            kmax > kw ? (kmax - kw) >> 6 : -1, A.tp, A.cr_scale, rck);
       } else if (la || lb) {
         const int u = la ? t : t + 1;
         const float hs[1] = {__shfl_sync(0xffffffffu, hs2, u)};
@@ -603,14 +626,10 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const float sc[1] = {__shfl_sync(0xffffffffu, tsc, u)};
         const uint32_t rb[1] = {la ? rb0 : rb0 + (uint32_t)RP};
         const int kk[1] = {la ? ka : kb};
-        if (kk[0] > kw)
-          sweep_masked_from<M, ST, WM, LOWC, OP, 1, TAPER, CURVED>(
-              acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c, lo_c, kw, lane, (kk[0] - kw) >> 6,
-              A.tp, A.cr_scale, rck);
-        else
-          sweep_traces<M, ST, WM, LOWC, false, OP, 1, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
-                                                              hi_c, lo_c, kw, lane, 0, A.tp,
-                                                              A.cr_scale, rck);
+        const int g = kk[0] > kw ? (kk[0] - kw) >> 6 : -1;
+        sweep_split<M, ST, WM, LOWC, OP, 1, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
+                                                           hi_c, lo_c, kw, lane, g, g, A.tp,
+                                                           A.cr_scale, rck);
       }
       const int adv = pair ? 2 : 1;
       t += adv;
@@ -657,7 +676,13 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         const int qc = qil * A.n_xl + qxl;
         int carry = 0;
         for (int base = 0; base < nk; base += 32) {
-          int v = (base + lane < nk) ? hist[warp * T + base + lane] : 0;
+          int v = 0;
+          if (base + lane < nk) {
+            const int e = warp * T + base + lane;
+            v = h16 ? (int)((reinterpret_cast<const unsigned*>(hist)[e >> 1] >> (16 * (e & 1))) &
+                            0xffffu)
+                    : hist[e];
+          }
 #pragma unroll
           for (int o = 1; o < 32; o <<= 1) {
             const int u = __shfl_up_sync(0xffffffffu, v, o);
@@ -745,11 +770,12 @@ inline cudaError_t launch2_one(const Plan* p, const KArgs& A, cudaStream_t s) {
                   : pstm_gather2_kernel<COLS, WPC, M, ST, WM, false, OP, AA, TAPER, CURVED>;
   const int T = WPC * 64 * M;
   KArgs A2 = A;
+  const int hb = hist_entry_bytes(A.hist16 != 0);
   if (!ring_shape(COLS, T, p->row_stride, (int)sizeof(ST), &A2.ring_stages, &A2.ring_rows,
-                  smem_budget(COLS * WPC * 32)))
+                  smem_budget(COLS * WPC * 32), hb))
     return cudaErrorInvalidValue;
   const Smem2 L = smem2_layout(COLS, T, p->row_stride, (int)sizeof(ST), A2.ring_stages,
-                               A2.ring_rows);
+                               A2.ring_rows, hb);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)p->n_tiles, (unsigned)((p->grid.n_times + T - 1) / T));

@@ -47,6 +47,9 @@ struct Plan {
   int64_t* tile_off = nullptr;   // n_tiles + 1
   int* tile_list = nullptr;      // sorted trace indices per tile
   int64_t list_entries = 0;
+  // longest tile list; below 65536 the forward kernel's fold histogram
+  // counts in 16-bit halves (every count is at most the list length)
+  int64_t longest_list = INT64_MAX;
   void* traces = nullptr;        // n_traces x row_stride, storage dtype
   float* scales = nullptr;       // per sorted trace (BF16/F16), else nullptr
   float* accum = nullptr;        // adjoint accumulation rows (n_traces x row_stride f32)

@@ -570,6 +570,7 @@ static cudaError_t sort_tile_lists(Plan* p, const TileGeom& tg, cudaStream_t s) 
   constexpr int64_t kChunk = int64_t(1) << 24;
   int64_t cap = 0, longest = 0;
   for (int64_t t = 0; t < n_tiles; ++t) longest = std::max(longest, off[t + 1] - off[t]);
+  p->longest_list = longest;
   cap = std::min(off[n_tiles], std::max(kChunk, longest));
   if (cap <= 1 || cap > INT32_MAX) return cudaSuccess;  // order is only a speed hint
   constexpr int64_t kMaxSegs = 65535;                      // tiles per key launch
@@ -893,6 +894,7 @@ pstm_status pstm_plan_create(pstm_plan** out, const pstm_grid* g, const pstm_par
                            cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   p->list_entries = total;
+  if (total == 0) p->longest_list = 0;
   CUDA_TRY(dalloc(p, &p->tile_list, total, s));
   if (total > 0) {
     tile_fill_kernel<<<(unsigned)p->n_tiles, 256, 0, s>>>(tg, cg, cell_start, p->geo, p->tile_off,
