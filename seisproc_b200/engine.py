@@ -80,6 +80,7 @@ class MigrationEngine:
         self.last_stats = {}
         self._stage, self._stage_key, self._pool = [], None, None
         self._copy_stream = None
+        self._plan_stream = None
         # bins of at least 2 x block_traces traces are uploaded and migrated in
         # up to max_blocks blocks (one plan each), pipelining the copies
         self.block_traces = 100_000
@@ -367,11 +368,12 @@ class MigrationEngine:
         the host-to-device copy behind the kernels.  The partial images and
         folds are summed on the device."""
         if blocks is None:
-            n_blk = min(self.max_blocks, max(1, n_tr // self.block_traces))
-            cuts = np.linspace(0, n_tr, n_blk + 1).astype(np.int64)
-            blocks = [(int(a), int(b - a)) for a, b in zip(cuts[:-1], cuts[1:])]
+            blocks = self._trace_blocks(n_tr)
         t_start = time.perf_counter()
         n_t = int(n_times) if n_times is not None else n_s
+        # the result arrays are allocated now and their pages faulted in by
+        # host threads while the kernels run
+        outs, faults = self._output_arrays((n_t, n_il, n_xl))
         if progress_callback:
             progress_callback(0.0, "Preparing data...")
         with torch.cuda.device(self.device):
@@ -426,25 +428,47 @@ class MigrationEngine:
                                                            if k != "variant"})
             plans = []
             try:
-                # every plan is built before the first launch (the builds
-                # synchronise this stream, which is idle until then)
-                for first, count in blocks:
-                    plans.append(PSTMPlan(*[c[first:first + count] for c in coords], **kw))
+                # Block 0's plan is built on this stream before the first launch;
+                # the plan of block b + 1 is built on a side stream while block b
+                # migrates (a build synchronises the stream it runs on, so on
+                # this stream it would wait for the kernels queued before it).
+                coords_ready = torch.cuda.Event()
+                coords_ready.record(cur)
+                if self._plan_stream is None:
+                    # high priority: the builds' small kernels take SMs as soon
+                    # as CTAs of the running migration retire
+                    self._plan_stream = torch.cuda.Stream(self.device, priority=-1)
+
+                def build(b):
+                    first, count = blocks[b]
+                    part = [c[first:first + count] for c in coords]
+                    if b == 0:
+                        return PSTMPlan(*part, **kw)
+                    self._plan_stream.wait_event(coords_ready)
+                    with torch.cuda.stream(self._plan_stream):
+                        plan = PSTMPlan(*part, **kw)
+                    for c in part:
+                        c.record_stream(self._plan_stream)
+                    return plan
+
+                plans.append(build(0))
                 if progress_callback:
                     progress_callback(0.1, "Running Kirchhoff migration...")
                 ev0 = torch.cuda.Event(enable_timing=True)
                 ev1 = torch.cuda.Event(enable_timing=True)
                 image = fold = None
-                for plan, wait in zip(plans, waits):
+                for b, wait in enumerate(waits):
                     tr, trace_major = wait()
                     if image is None:
                         ev0.record()
-                    img_b, fold_b = plan.migrate(tr, vel_t, trace_major=trace_major)
+                    img_b, fold_b = plans[b].migrate(tr, vel_t, trace_major=trace_major)
                     if image is None:
                         image, fold = img_b, fold_b
                     else:
                         image.add_(img_b)
                         fold.add_(fold_b)
+                    if b + 1 < len(blocks):
+                        plans.append(build(b + 1))
                 ev1.record()
                 for plan in plans:
                     plan.check()
@@ -467,38 +491,82 @@ class MigrationEngine:
             if normalize:
                 from .kirchhoff import normalize_by_fold
                 image = normalize_by_fold(image, fold, min_fold)
-            image_np, fold_np = self._download(image, fold)
+            image_np, fold_np = self._download(image, fold, outs, faults)
         logger.info("Full migration complete: %.2fs", time.perf_counter() - t_start)
         if progress_callback:
             progress_callback(1.0, "Complete")
         return image_np, fold_np
 
-    def _download(self, image: torch.Tensor, fold: torch.Tensor) -> Tuple[np.ndarray, np.ndarray]:
-        """Device results to new numpy arrays.
+    def _trace_blocks(self, n_tr: int):
+        """Blocks of traces (first, count) for a bin: up to ``max_blocks``, the
+        first one an eighth of the bin when there are several, so that the
+        first launch waits for a small upload; the rest split the remainder."""
+        n_blk = min(self.max_blocks, max(1, n_tr // self.block_traces))
+        if n_blk == 1:
+            return [(0, n_tr)]
+        first = n_tr // (2 * n_blk)
+        cuts = first + np.linspace(0, n_tr - first, n_blk).astype(np.int64)
+        cuts = np.concatenate([[0], cuts])
+        return [(int(a), int(b - a)) for a, b in zip(cuts[:-1], cuts[1:])]
+
+    def _workers(self):
+        if self._pool is None:
+            import concurrent.futures as cf
+            self._pool = cf.ThreadPoolExecutor(max_workers=8)
+        return self._pool
+
+    def _output_arrays(self, shape):
+        """Two new float32 arrays of ``shape`` (image, fold) and the futures of
+        the host threads that touch every page of them (a first touch faults
+        the page in, which costs more than the bus transfer into it)."""
+        outs = [np.empty(shape, np.float32) for _ in range(2)]
+        flat = [o.reshape(-1) for o in outs]
+        cuts = np.linspace(0, flat[0].shape[0], 5).astype(np.int64)
+        pool = self._workers()
+        faults = [pool.submit(f[a:b].fill, 0.0) for f in flat for a, b in zip(cuts[:-1], cuts[1:])]
+        return outs, faults
+
+    def _download(self, image: torch.Tensor, fold: torch.Tensor, outs=None,
+                  faults=()) -> Tuple[np.ndarray, np.ndarray]:
+        """Device results to numpy arrays (new ones unless ``outs`` is given,
+        whose page faulting ``faults`` are the futures of).
 
         Both come back through page-locked staging buffers kept by the engine
         (a copy straight into pageable memory runs at a fraction of the bus
-        bandwidth).  The fresh arrays fault their pages in on first touch, which
-        costs more than the bus transfer, so the copies out of staging are
-        split into slices over eight threads."""
+        bandwidth), in four slices each: host threads copy a slice out of
+        staging as soon as its transfer has landed, while the next ones cross
+        the bus."""
         key = tuple(image.shape)
         if self._stage_key != key:
             self._stage = [torch.empty(key, dtype=torch.float32, pin_memory=True) for _ in range(2)]
             self._stage_key = key
-        for h, d in zip(self._stage, (image, fold)):
-            h.copy_(d, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
-        outs = [np.empty(key, np.float32) for _ in range(2)]
-        if self._pool is None:
-            import concurrent.futures as cf
-            self._pool = cf.ThreadPoolExecutor(max_workers=8)
+        if outs is None:
+            outs, faults = self._output_arrays(key)
+        n = outs[0].size
+        cuts = np.linspace(0, n, 5).astype(np.int64)
+        dev = [image.reshape(-1), fold.reshape(-1)]
+        stage = [h.reshape(-1) for h in self._stage]
         src = [h.numpy().reshape(-1) for h in self._stage]
         dst = [o.reshape(-1) for o in outs]
-        n = dst[0].shape[0]
-        cuts = np.linspace(0, n, 5).astype(np.int64)
-        jobs = [(i, a, b) for i in range(2) for a, b in zip(cuts[:-1], cuts[1:])]
-        list(self._pool.map(lambda j: np.copyto(dst[j[0]][j[1]:j[2]], src[j[0]][j[1]:j[2]]),
-                            jobs))
+        pool = self._workers()
+        for f in faults:
+            f.result()
+
+        def copy_out(ev, i, a, b):
+            while not ev.query():  # polls, so the waiting threads hold no lock
+                time.sleep(2e-4)
+            np.copyto(dst[i][a:b], src[i][a:b])
+
+        jobs = []
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            for i in range(2):
+                stage[i][a:b].copy_(dev[i][a:b], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record()
+                jobs.append(pool.submit(copy_out, ev, i, int(a), int(b)))
+        for j in jobs:
+            j.result()
+        torch.cuda.current_stream().synchronize()
         return outs[0], outs[1]
 
     def _not_this_operator(self, name: str):
