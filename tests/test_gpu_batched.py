@@ -136,7 +136,8 @@ def test_from_survey_matches_per_class_plans():
 
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
 def test_engine_migrate_bins_full_matches_per_bin_calls(storage):
-    """MigrationEngine.migrate_bins_full (every bin in one batched launch) gives
+    """MigrationEngine.migrate_bins_full (the bins in pipelined groups of
+    batched launches: one bin per group, then every bin in one group) gives
     each bin the image and fold that migrate_bin_full gives it alone, into new
     arrays or into the caller's page-locked buffers."""
     from seisproc_b200.engine import MigrationEngine
@@ -156,6 +157,7 @@ def test_engine_migrate_bins_full_matches_per_bin_calls(storage):
     shape = (s0.n_times, s0.n_il, s0.n_xl)
     outs = [(torch.empty(shape, pin_memory=True), torch.empty(shape, pin_memory=True))
             for _ in bins]
+    eng.batch_groups = 1
     res2 = eng.migrate_bins_full(bins, out=outs, **kw)
     for b, (img, fold), (img2, fold2) in zip(bins, res, res2):
         ri, rf = eng.migrate_bin_full(b["traces"], b["source_x"], b["source_y"],
