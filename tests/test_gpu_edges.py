@@ -79,3 +79,32 @@ def test_traces_too_long_for_the_staged_kernel():
         PSTMPlan(*c, n_il=4, n_xl=4, n_times=100, origin_x=0.0, origin_y=0.0, il_dx=25.0,
                  il_dy=0.0, xl_dx=0.0, xl_dy=25.0, t0_ms=0.0, dt_ms=4.0, n_samples=60000,
                  in_t0_ms=0.0, in_dt_ms=4.0, max_aperture_m=500.0, max_angle_deg=60.0)
+
+
+@pytest.mark.parametrize("variant", [1, 3])
+@pytest.mark.parametrize("n_tr", [65535, 65536])
+def test_fold_counts_of_a_full_tile_list(n_tr, variant):
+    """Every trace at one point, so one tile list holds all of them and each
+    column's fold histogram takes n_tr counts in one bin: 65535 traces use the
+    16-bit counts, 65536 the 32-bit histogram; the fold is exact either way."""
+    from seisproc_b200.kirchhoff import PSTMPlan
+    dev = torch.device("cuda")
+    n_s = n_t = 64
+    # the point sits between the 2 x 2 columns, 17.7 m from each: with
+    # V = 2000 m/s and dt = 4 ms, z = 4 k m, so tan(60) z exceeds 17.7 m from
+    # sample 3 on (13.9 m at sample 2, 20.8 m at sample 3)
+    p = np.full(n_tr, 1012.5)
+    c = [torch.from_numpy(p.copy()).to(dev) for _ in range(4)]
+    plan = PSTMPlan(*c, n_il=2, n_xl=2, n_times=n_t, origin_x=1000.0, origin_y=1000.0,
+                    il_dx=25.0, il_dy=0.0, xl_dx=0.0, xl_dy=25.0, t0_ms=0.0, dt_ms=4.0,
+                    n_samples=n_s, in_t0_ms=0.0, in_dt_ms=4.0, max_aperture_m=500.0,
+                    max_angle_deg=60.0, forward_only=True, variant=variant)
+    assert plan.stats()["list_entries"] == n_tr
+    tr = torch.from_numpy(np.random.RandomState(n_tr).standard_normal((n_s, n_tr))
+                          .astype(np.float32)).to(dev)
+    img, fold = plan.migrate(tr, torch.full((n_t,), 2000.0, device=dev))
+    plan.check()
+    plan.close()
+    fold = fold.reshape(n_t, -1).cpu().numpy()
+    assert (fold[:3] == 0).all() and (fold[3:] == n_tr).all()
+    assert torch.isfinite(img).all()

@@ -140,3 +140,18 @@ def test_offset_taper_matches_reference_controller():
     for k in range(2):
         tw, _, _, omin, omax = g[f"params{k}"]
         assert np.allclose(offset_taper(off, omin, omax, tw), g[f"offset_mask{k}"], atol=2e-6)
+
+
+def test_engine_trace_blocks():
+    """A bin's blocks of traces tile it exactly; several blocks start with one
+    an eighth of the bin (its upload is all the first launch waits for)."""
+    from seisproc_b200.engine import MigrationEngine
+    eng = MigrationEngine.__new__(MigrationEngine)  # no device needed for the split
+    eng.block_traces, eng.max_blocks = 100_000, 4
+    for n in (0, 5, 150_000, 200_000, 500_000, 1_000_003):
+        blocks = eng._trace_blocks(n)
+        assert blocks[0][0] == 0 and sum(c for _, c in blocks) == n
+        assert all(a + c == b for (a, c), (b, _) in zip(blocks, blocks[1:]))
+        assert len(blocks) == min(4, max(1, n // 100_000))
+        if len(blocks) > 1:
+            assert blocks[0][1] == n // (2 * len(blocks))
