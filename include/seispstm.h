@@ -359,11 +359,11 @@ int64_t pstm_launch_count(void);
  * worst case, 4 B per tile per trace) and the staged float32 trace rows;
  * storage must be PSTM_F32.  Non-finite coordinates reject with PSTM_EINVAL, as
  * in pstm_plan_create.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress), so make it before any stream capture.
- * All calls share the array: calls whose work overlaps on the GPU race, and
- * the array keeps the last call's contents (the error flag is cleared on every
- * call).  The call synchronises `stream` before it returns, to report
- * device-side errors. */
+ * device address (cudaGetSymbolAddress).  All calls share the array: calls
+ * whose work overlaps on the GPU race, and the array keeps the last call's
+ * contents (the error flag is cleared on every call).  The call synchronises
+ * `stream` before it returns, to report device-side errors, so it cannot be
+ * captured in a CUDA graph (a plan with pstm_migrate can). */
 pstm_status pstm_migrate_noalloc(const pstm_grid* grid, const pstm_params* params,
                                  const pstm_geometry* geometry, const float* traces,
                                  const float* velocity, int64_t v_stride_t, int64_t v_stride_c,

@@ -12,8 +12,9 @@
 //
 // The host-side symbol of the array is only a stand-in for the device object:
 // its device address is obtained once per device with cudaGetSymbolAddress
-// (with that device current) and passed to the kernels.  The first call on a
-// device performs that lookup, so it should happen before any stream capture.
+// (with that device current) and passed to the kernels; the first call on a
+// device performs that lookup.  Every call reads the device error flag back
+// and synchronises its stream, so the call cannot be captured in a CUDA graph.
 // All calls share the one array and it keeps the previous call's contents;
 // everything that must start at zero (the error flag) is cleared on each call,
 // and calls whose work overlaps on the GPU race on the array.
