@@ -51,7 +51,7 @@ int test_injection() { return g_inject.load(std::memory_order_relaxed); }
 // ---------------------------------------------------------------------------
 template <int COLS, int T>
 __global__ void __launch_bounds__(256) pstm_fold_kernel(const KArgs A) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   float* thr = reinterpret_cast<float*>(smem);
   int* hist = reinterpret_cast<int*>(smem + COLS * T * 4);
   const int tile = blockIdx.x;
