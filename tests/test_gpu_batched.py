@@ -233,3 +233,40 @@ def test_short_window_shapes_match_default_shape(shape):
     assert rel_l2(ai.cpu().numpy(), ri.cpu().numpy()) <= 1e-5
     for p in plans + [ref, alt]:
         p.close()
+
+
+def test_batched_fold_with_a_long_tile_list():
+    """A batch where one class's tile list holds 70 000 traces takes the 32-bit
+    fold histogram for every class (one shared-memory layout per launch); the
+    folds and images equal the per-class launches, which choose their
+    histograms alone (16-bit for the small class)."""
+    from seisproc_b200.batched import BatchedPSTM
+    from seisproc_b200.kirchhoff import PSTMPlan
+    dev = torch.device("cuda")
+    n_s = n_t = 64
+    rs = np.random.RandomState(70)
+    plans, traces = [], []
+    for n in (70000, 500):
+        # every trace near one point between the 2 x 2 columns
+        c = [torch.from_numpy(1012.5 + rs.uniform(-5.0, 5.0, n)).to(dev) for _ in range(4)]
+        plans.append(PSTMPlan(*c, n_il=2, n_xl=2, n_times=n_t, origin_x=1000.0,
+                              origin_y=1000.0, il_dx=25.0, il_dy=0.0, xl_dx=0.0, xl_dy=25.0,
+                              t0_ms=0.0, dt_ms=4.0, n_samples=n_s, in_t0_ms=0.0, in_dt_ms=4.0,
+                              max_aperture_m=500.0, max_angle_deg=60.0, forward_only=True,
+                              variant=1))
+        traces.append(torch.from_numpy(rs.standard_normal((n_s, n)).astype(np.float32)).to(dev))
+    assert plans[0].stats()["list_entries"] == 70000
+    v = torch.full((n_t,), 2000.0, device=dev)
+    b = BatchedPSTM(plans, v)
+    b.load(traces)
+    b.migrate()
+    b.check()
+    for p, tr, img, fold in zip(plans, traces, b.images, b.folds):
+        ri, rf = p.migrate(tr, v)
+        p.check()
+        assert torch.equal(fold, rf)
+        assert torch.equal(img, ri)
+    assert float(b.folds[0].max()) == 70000.0
+    b.close()
+    for p in plans:
+        p.close()
