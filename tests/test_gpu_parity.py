@@ -344,3 +344,88 @@ def test_plans_reuse_pooled_memory_and_trim():
     seisproc_b200.release_cached_memory(1 << 30)
     with pytest.raises(ValueError):
         seisproc_b200.release_cached_memory(-1)
+
+
+@pytest.mark.parametrize("forward_only", [False, True])
+def test_linearity_in_the_traces(forward_only):
+    """The operator is linear in the trace samples: scaling the traces by a
+    power of two scales the image exactly (no rounding enters: the staged rows,
+    the interpolation and every partial sum scale with them), a sum of two
+    trace sets migrates to the sum of their images within float32 rounding,
+    and the fold does not depend on the samples.  Rows in intercept form
+    (forward_only plans) interpolate as idx * slope + intercept, whose terms
+    are up to a trace length larger than the sample, so their rounding is
+    ~1e-5 of the image (within the 1e-4 parity tolerance); (x, dx) rows round
+    at ~1e-7."""
+    from seisproc_b200 import synthetic
+    from seisproc_b200.kirchhoff import PSTMPlan
+    dev = torch.device("cuda")
+    s = synthetic.survey_3d(n_traces=40000, seed=11, n_samples=500, dt_ms=2.0, extent=2000.0,
+                            max_offset=1500.0, n_il=64, n_xl=64, spacing=25.0, n_diffractors=20,
+                            aperture=800.0)
+    c = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    plan = PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=s.origin_x,
+                    origin_y=s.origin_y, il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0,
+                    xl_dy=s.xl_spacing, t0_ms=0.0, dt_ms=s.dt_ms, n_samples=s.n_samples,
+                    in_t0_ms=0.0, in_dt_ms=s.dt_ms, max_aperture_m=s.max_aperture_m,
+                    max_angle_deg=s.max_angle_deg, forward_only=forward_only)
+    v = torch.from_numpy(s.vrms).to(dev)
+    g = torch.Generator(device=dev).manual_seed(11)
+    x = torch.randn((s.n_samples, s.n_traces), device=dev, generator=g)
+    y = torch.randn((s.n_samples, s.n_traces), device=dev, generator=g)
+    lx, fx = plan.migrate(x, v)
+    lx = lx.clone()
+    l4, f4 = plan.migrate(4.0 * x, v)
+    assert torch.equal(l4, 4.0 * lx) and torch.equal(f4, fx)
+    ly, _ = plan.migrate(y, v)
+    ly = ly.clone()
+    lxy, fxy = plan.migrate(x + y, v)
+    plan.check()
+    plan.close()
+    assert torch.equal(fxy, fx)
+    tol = 5e-5 if forward_only else 1e-6
+    assert rel_l2(lxy.cpu().numpy(), (lx + ly).cpu().numpy()) <= tol
+
+
+def test_reciprocity_and_translation():
+    """Swapping every trace's source and receiver leaves the fold unchanged
+    exactly and the image within float32 rounding (the traveltime, masks and
+    weight are symmetric in the two legs, but the legs are summed in the other
+    order: the float32 index moves by up to an ulp, 6e-5 of a sample at sample
+    1000, which white-noise traces turn into ~1e-5 of the image, inside the
+    1e-4 parity tolerance); moving the survey and the grid by a
+    whole kilometre-scale offset leaves both bit for bit unchanged (the origin
+    is subtracted in float64 before the float32 geometry is formed)."""
+    from seisproc_b200 import synthetic
+    from seisproc_b200.kirchhoff import PSTMPlan
+    dev = torch.device("cuda")
+    s = synthetic.survey_3d(n_traces=20000, seed=12, n_samples=400, dt_ms=2.0, extent=1600.0,
+                            max_offset=1500.0, n_il=48, n_xl=40, spacing=25.0, n_diffractors=12,
+                            aperture=700.0)
+    v = torch.from_numpy(s.vrms).to(dev)
+    tr = torch.from_numpy(np.random.RandomState(12).standard_normal(
+        (s.n_samples, s.n_traces)).astype(np.float32)).to(dev)
+
+    def run(sx, sy, rx, ry, ox, oy):
+        c = [torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+             for a in (sx, sy, rx, ry)]
+        p = PSTMPlan(*c, n_il=s.n_il, n_xl=s.n_xl, n_times=s.n_times, origin_x=ox, origin_y=oy,
+                     il_dx=s.il_spacing, il_dy=0.0, xl_dx=0.0, xl_dy=s.xl_spacing, t0_ms=0.0,
+                     dt_ms=s.dt_ms, n_samples=s.n_samples, in_t0_ms=0.0, in_dt_ms=s.dt_ms,
+                     max_aperture_m=s.max_aperture_m, max_angle_deg=s.max_angle_deg)
+        img, fold = p.migrate(tr, v)
+        p.check()
+        p.close()
+        return img.cpu().numpy(), fold.cpu().numpy()
+
+    # coordinates on a 1/1024 m grid, so that the shifted ones are exact in float64
+    g = [np.round(np.asarray(a, np.float64) * 1024.0) / 1024.0
+         for a in (s.source_x, s.source_y, s.receiver_x, s.receiver_y)]
+    img, fold = run(*g, s.origin_x, s.origin_y)
+    assert fold.sum() > 0
+    ri, rf = run(g[2], g[3], g[0], g[1], s.origin_x, s.origin_y)
+    assert np.array_equal(rf, fold) and rel_l2(ri, img) <= 3e-5
+    dx, dy = 512000.0, 6144000.0  # UTM-sized
+    ti, tf = run(g[0] + dx, g[1] + dy, g[2] + dx, g[3] + dy, s.origin_x + dx, s.origin_y + dy)
+    assert np.array_equal(tf, fold) and np.array_equal(ti, img)
