@@ -566,9 +566,13 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
     const int pn = p0 + 32 + lane;
     if (pn < n_list) jj_next = list_entry(A, off0 + pn);
     const int nt = min(32, n_list - p0);
+    bool prefetched = false;  // the next chunk's geometry is loaded a few traces in
     for (int t = 0; t < nt;) {
       const int p = p0 + t;
-      if (t <= 4 && t + 2 > 4 && warp_live && pn < n_list) g_next = __ldg(A.geo + jj_next);
+      if (!prefetched && t >= 4) {
+        if (warp_live && pn < n_list) g_next = __ldg(A.geo + jj_next);
+        prefetched = true;
+      }
       if (slot == 0) {
         bool ok = true;
         if (lane == 0) ok = mbar_wait(full + stage, phase);
@@ -582,13 +586,14 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
           break;
         }
       }
-      // two traces of the same stage when available
-      const bool pair = (slot + 1 < B) && (t + 1 < nt);
-      const int ka = __shfl_sync(0xffffffffu, ks, t);
-      const int kb = __shfl_sync(0xffffffffu, ks, pair ? t + 1 : t);
-      const bool la = ka < kwe, lb = pair && kb < kwe;
-      const uint32_t rb0 = raw_base + (uint32_t)((stage * B + slot) * RP);
+      int adv;
       if constexpr (AA) {
+        // two traces of the same stage when available
+        const bool pair = (slot + 1 < B) && (t + 1 < nt);
+        const int ka = __shfl_sync(0xffffffffu, ks, t);
+        const int kb = __shfl_sync(0xffffffffu, ks, pair ? t + 1 : t);
+        const bool la = ka < kwe, lb = pair && kb < kwe;
+        const uint32_t rb0 = raw_base + (uint32_t)((stage * B + slot) * RP);
         // anti-aliased sweeps take one trace at a time (three taps per sample)
         for (int q = 0; q < (pair ? 2 : 1); ++q) {
           const int u = t + q;
@@ -609,29 +614,47 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
             sweep_aa<M, LOWC, false, 1>(acc, zz, aa, hs, hr, g0, g1, g2, g3, rb, kk, bb, mg, hi_c,
                                         lo_c, A.aa_lmax, kw, lane, 0, rck);
         }
-      } else if (la && lb) {
-        const float hs[2] = {__shfl_sync(0xffffffffu, hs2, t), __shfl_sync(0xffffffffu, hs2, t + 1)};
-        const float hr[2] = {__shfl_sync(0xffffffffu, hr2, t), __shfl_sync(0xffffffffu, hr2, t + 1)};
-        const float sc[2] = {__shfl_sync(0xffffffffu, tsc, t), __shfl_sync(0xffffffffu, tsc, t + 1)};
-        const uint32_t rb[2] = {rb0, rb0 + (uint32_t)RP};
-        const int kk[2] = {ka, kb};
-        const int kmax = max(ka, kb);
-        sweep_split<M, ST, WM, LOWC, OP, 2, TAPER, CURVED>(
-            acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c, lo_c, kw, lane, (min(ka, kb) - kw) >> 6,
-            kmax > kw ? (kmax - kw) >> 6 : -1, A.tp, A.cr_scale, rck);
-      } else if (la || lb) {
-        const int u = la ? t : t + 1;
-        const float hs[1] = {__shfl_sync(0xffffffffu, hs2, u)};
-        const float hr[1] = {__shfl_sync(0xffffffffu, hr2, u)};
-        const float sc[1] = {__shfl_sync(0xffffffffu, tsc, u)};
-        const uint32_t rb[1] = {la ? rb0 : rb0 + (uint32_t)RP};
-        const int kk[1] = {la ? ka : kb};
-        const int g = kk[0] > kw ? (kk[0] - kw) >> 6 : -1;
-        sweep_split<M, ST, WM, LOWC, OP, 1, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb, mg,
-                                                           hi_c, lo_c, kw, lane, g, g, A.tp,
-                                                           A.cr_scale, rck);
+        adv = pair ? 2 : 1;
+      } else {
+        // the traces of this stage (within the chunk) that reach the warp's
+        // window, two at a time in list order; the others are skipped
+        const int t_end = min(nt, t + (B - slot));
+        const unsigned live = __ballot_sync(0xffffffffu, lane >= t && lane < t_end && ks < kwe);
+        if (live == 0) {
+          adv = t_end - t;
+        } else {
+          // staged row of chunk position u: slot + (u - t) of this stage
+          const uint32_t rbs = raw_base + (uint32_t)((stage * B + slot - t) * RP);
+          const int a = __ffs(live) - 1;
+          const unsigned rest = live & (live - 1);
+          const int ka = __shfl_sync(0xffffffffu, ks, a);
+          if (rest) {
+            const int b = __ffs(rest) - 1;
+            const int kb = __shfl_sync(0xffffffffu, ks, b);
+            const float hs[2] = {__shfl_sync(0xffffffffu, hs2, a), __shfl_sync(0xffffffffu, hs2, b)};
+            const float hr[2] = {__shfl_sync(0xffffffffu, hr2, a), __shfl_sync(0xffffffffu, hr2, b)};
+            const float sc[2] = {__shfl_sync(0xffffffffu, tsc, a), __shfl_sync(0xffffffffu, tsc, b)};
+            const uint32_t rb[2] = {rbs + (uint32_t)(a * RP), rbs + (uint32_t)(b * RP)};
+            const int kk[2] = {ka, kb};
+            const int kmax = max(ka, kb);
+            sweep_split<M, ST, WM, LOWC, OP, 2, TAPER, CURVED>(
+                acc, zz, aa, hs, hr, rb, kk, sc, bb, mg, hi_c, lo_c, kw, lane,
+                (min(ka, kb) - kw) >> 6, kmax > kw ? (kmax - kw) >> 6 : -1, A.tp, A.cr_scale, rck);
+            adv = b + 1 - t;
+          } else {
+            const float hs[1] = {__shfl_sync(0xffffffffu, hs2, a)};
+            const float hr[1] = {__shfl_sync(0xffffffffu, hr2, a)};
+            const float sc[1] = {__shfl_sync(0xffffffffu, tsc, a)};
+            const uint32_t rb[1] = {rbs + (uint32_t)(a * RP)};
+            const int kk[1] = {ka};
+            const int g = ka > kw ? (ka - kw) >> 6 : -1;
+            sweep_split<M, ST, WM, LOWC, OP, 1, TAPER, CURVED>(acc, zz, aa, hs, hr, rb, kk, sc, bb,
+                                                               mg, hi_c, lo_c, kw, lane, g, g,
+                                                               A.tp, A.cr_scale, rck);
+            adv = t_end - t;
+          }
+        }
       }
-      const int adv = pair ? 2 : 1;
       t += adv;
       slot += adv;
       if (slot == B || p + adv == n_list) {
@@ -659,6 +682,7 @@ __device__ __forceinline__ void gather_tile(const KArgs& A, const int tile, cons
         }
       }
     }
+    if (!prefetched && warp_live && pn < n_list) g_next = __ldg(A.geo + jj_next);
   }
   if (aborted) {
     // leave no bulk copy in flight into this CTA's shared memory
